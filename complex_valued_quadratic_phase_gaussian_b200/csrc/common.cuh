@@ -1,0 +1,123 @@
+// Shared device helpers for the CVQPG B200 kernels (sm_100a).
+//
+// Everything here is header-only and used by several translation units:
+// status codes, launch helpers, complex arithmetic, the range-reduced sincos
+// used by the splat, and a counter-based normal generator for the loss noise.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/cvqpg.h"
+
+namespace cvqpg {
+
+constexpr int kTile = 16;                 // splat tile edge in pixels (cuda/config.h BLOCK_X/Y)
+constexpr int kTilePixels = kTile * kTile;
+constexpr int kMaxChannels = 3;
+
+// Launch-error check used by every C-ABI entry point after its launches.
+static inline int launch_status() {
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CVQPG_OK : CVQPG_ERR_CUDA;
+}
+
+static inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+// Bump-pointer carving of a caller-provided workspace into 256-byte aligned slices.
+struct Carver {
+    char* base;
+    size_t off;
+    size_t cap;
+    explicit Carver(void* p, size_t c) : base((char*)p), off(0), cap(c) {}
+    template <typename T>
+    T* take(size_t count) {
+        off = (off + 255) & ~(size_t)255;
+        T* p = base ? (T*)(base + off) : nullptr;
+        off += count * sizeof(T);
+        return p;
+    }
+    bool fits() const { return off <= cap; }
+};
+
+// ---------------------------------------------------------------------------
+// complex helpers (float2 = re, im)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// ---------------------------------------------------------------------------
+// sincos with an FMA Cody-Waite reduction modulo 2*pi.
+//
+// Method: W. J. Cody and W. Waite, "Software Manual for the Elementary
+// Functions" (1980), additive range reduction with a two-term constant; the
+// FMA form follows J.-M. Muller, "Elementary Functions" (3rd ed., 2016), sec. 11.
+// The reduced argument lies in [-pi, pi], where the hardware sin/cos
+// approximations (MUFU) have an absolute error below 2^-21.4. The splat phase
+// phi + k*base is unbounded, so reducing first keeps the error at ~1e-7 rad for
+// any |x| below ~1e6 instead of growing with |x|.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sincos_reduced(float x, float* s, float* c) {
+    const float kInv2Pi = 0.15915494309189535f;
+    const float k2PiHi = 6.28318548202514648f;       // float(2*pi)
+    const float k2PiLo = -1.7484555314695172e-07f;   // 2*pi - float(2*pi)
+    const float n = rintf(x * kInv2Pi);
+    float r = fmaf(-n, k2PiHi, x);
+    r = fmaf(-n, k2PiLo, r);
+    __sincosf(r, s, c);
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 counter-based generator (J. K. Salmon, M. A. Moraes, R. O. Dror,
+// D. E. Shaw, "Parallel Random Numbers: As Easy as 1, 2, 3", SC 2011) and a
+// Box-Muller transform to standard normals. Used for the fresh target noise of
+// the multi-plane loss; the oracle restates the same generator.
+// ---------------------------------------------------------------------------
+struct Philox4 {
+    uint32_t v[4];
+};
+
+__host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                         uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)M0 * c0;
+        uint64_t p1 = (uint64_t)M1 * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n1 = lo1;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        uint32_t n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += W0; k1 += W1;
+    }
+    Philox4 o;
+    o.v[0] = c0; o.v[1] = c1; o.v[2] = c2; o.v[3] = c3;
+    return o;
+}
+
+// Uniform in (0, 1]: (u + 1) * 2^-32 computed exactly in double then rounded.
+__device__ __forceinline__ float u32_to_open01(uint32_t u) {
+    return (float)(((double)u + 1.0) * 2.3283064365386963e-10);
+}
+
+// One standard normal for element `idx` of stream (`seed`, `offset`).
+// Box-Muller on the first two Philox words: z = sqrt(-2 ln u1) cos(2 pi u2).
+__device__ __forceinline__ float normal_at(uint64_t seed, uint64_t offset, uint64_t idx) {
+    Philox4 r = philox4x32_10((uint32_t)idx, (uint32_t)(idx >> 32), (uint32_t)offset, (uint32_t)(offset >> 32),
+                              (uint32_t)seed, (uint32_t)(seed >> 32));
+    const float u1 = u32_to_open01(r.v[0]);
+    const float u2 = u32_to_open01(r.v[1]);
+    const float rad = sqrtf(-2.0f * logf(u1));
+    return rad * cospif(2.0f * u2);
+}
+
+}  // namespace cvqpg

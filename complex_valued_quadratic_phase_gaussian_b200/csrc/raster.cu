@@ -1,0 +1,768 @@
+// Tile binning and the complex quadratic-phase splat (forward and adjoint).
+//
+// Binning (reference: cuda/forward.cu:8-60, cuda/raster.cu:60-95):
+//   tiles_touched -> inclusive scan -> (tile, id) pairs in id order -> stable
+//   LSD radix sort on the tile bits only -> per-tile [start, end) ranges.
+// The reference sorts 64-bit (tile<<32 | id) keys over all 64 bits; because the
+// pairs are emitted in ascending id and an LSD radix sort is stable, sorting
+// the ceil(log2 T) tile bits gives the identical permutation with 1-2 passes
+// instead of 8. The pair count stays on the device (no host round trip), so
+// every stage can be captured in a CUDA graph; buffers are sized by a caller
+// capacity and an overflow flag reports when it was too small.
+//
+// Splat (reference: cuda/forward.cu:63-162 forward, cuda/backward.cu:22-168
+// adjoint): linear coherent sum
+//   U_c(p) = sum_g A_gc * o_g * G_g(p) * exp(i (phi_gc + k_c * 0.5 * c_g * m_g(p) * area_g * dxy2))
+// with m = Mahalanobis distance and G = exp(max(-m/2, -50)).
+#include "raster.cuh"
+
+namespace cvqpg {
+
+// ---------------------------------------------------------------------------
+// record packing for the drop-in entry point (reference SoA tensors -> records)
+// ---------------------------------------------------------------------------
+template <int C>
+__global__ void pack_records_kernel(int n, const float* __restrict__ means, const float* __restrict__ inv_cov,
+                                    const float* __restrict__ colours, const float* __restrict__ phase,
+                                    const float* __restrict__ opac, const float* __restrict__ curv,
+                                    const float* __restrict__ area, float* __restrict__ rec) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    float v[kRecordFloats];
+    v[0] = means[2 * g];
+    v[1] = means[2 * g + 1];
+    v[2] = inv_cov[3 * g];
+    v[3] = inv_cov[3 * g + 1];
+    v[4] = inv_cov[3 * g + 2];
+    v[5] = opac[g];
+    v[6] = curv[g];
+    v[7] = area[g];
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        v[8 + c] = colours[g * C + c];
+        v[8 + C + c] = phase[g * C + c];
+    }
+#pragma unroll
+    for (int i = 8 + 2 * C; i < kRecordFloats; i++) v[i] = 0.0f;
+    float4* dst = reinterpret_cast<float4*>(rec + (size_t)g * kRecordFloats);
+#pragma unroll
+    for (int q = 0; q < 4; q++) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+static void launch_pack_records(int channels, int n, const float* means, const float* inv_cov, const float* colours,
+                                const float* phase, const float* opac, const float* curv, const float* area,
+                                float* rec, cudaStream_t stream) {
+    if (n <= 0) return;
+    if (channels == 1)
+        pack_records_kernel<1><<<ceil_div(n, 256), 256, 0, stream>>>(n, means, inv_cov, colours, phase, opac, curv,
+                                                                     area, rec);
+    else
+        pack_records_kernel<3><<<ceil_div(n, 256), 256, 0, stream>>>(n, means, inv_cov, colours, phase, opac, curv,
+                                                                     area, rec);
+}
+
+// reference preprocessKernel (cuda/forward.cu:15-26), generalised to the rule
+__global__ void tile_count_kernel(BinRule rule, const float* __restrict__ rec, int n,
+                                  uint32_t* __restrict__ tiles_touched) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const float2 m = *reinterpret_cast<const float2*>(rec + (size_t)g * kRecordFloats);
+    uint32_t cnt = 0;
+    for_each_list_tile(rule, m.x, m.y, g, [&](int) { cnt++; });
+    tiles_touched[g] = cnt;
+}
+
+BinRule make_bin_rule(int mode, int width, int height, const int32_t* radii, const float* radius_f) {
+    BinRule r;
+    r.mode = mode;
+    r.width = width;
+    r.height = height;
+    r.radii = radii;
+    r.radius_f = radius_f;
+    if (mode == CVQPG_CULL_CUDA16_5SIGMA) {
+        r.list_tile = kTile;
+    } else if (mode == CVQPG_CULL_TORCH64_3SIGMA) {
+        r.list_tile = 64;
+    } else {
+        r.list_tile = 0;
+    }
+    if (r.list_tile > 0) {
+        r.lgx = (width + r.list_tile - 1) / r.list_tile;
+        r.lgy = (height + r.list_tile - 1) / r.list_tile;
+    } else {
+        r.lgx = 1;
+        r.lgy = 1;
+    }
+    return r;
+}
+
+void launch_tile_count(const BinRule& rule, const float* records, int n, uint32_t* tiles_touched,
+                       cudaStream_t stream) {
+    if (n <= 0) return;
+    tile_count_kernel<<<ceil_div(n, 256), 256, 0, stream>>>(rule, records, n, tiles_touched);
+}
+
+// ---------------------------------------------------------------------------
+// inclusive scan of tiles_touched (reduce, scan of block sums, downsweep)
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 4;
+constexpr int kScanBlock = kScanThreads * kScanItems;  // 1024
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t warp_sums[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t s = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        warp_sums[lane] = s;  // inclusive over warps
+    }
+    __syncthreads();
+    const uint32_t warp_prefix = w > 0 ? warp_sums[w - 1] : 0;
+    if (total) *total = warp_sums[nw - 1];
+    const uint32_t excl = warp_prefix + x - v;
+    __syncthreads();
+    return excl;
+}
+
+__global__ void scan_reduce_kernel(int n, const uint32_t* __restrict__ in, uint32_t* __restrict__ partials) {
+    const int base = blockIdx.x * kScanBlock;
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const int idx = base + i * kScanThreads + threadIdx.x;
+        if (idx < n) s += in[idx];
+    }
+    uint32_t total;
+    block_exclusive_scan(s, &total);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+// Single block: exclusive scan of the block sums; writes the pair count and the
+// overflow flag. pair_count[0] is clamped to the capacity.
+__global__ void scan_partials_kernel(int nblocks, uint32_t* __restrict__ partials, int cap,
+                                     int32_t* __restrict__ pair_count) {
+    // each thread handles a contiguous chunk of ceil(nblocks/blockDim) partials
+    const int per = (nblocks + blockDim.x - 1) / blockDim.x;
+    const int b0 = threadIdx.x * per;
+    uint32_t local = 0;
+    for (int i = 0; i < per; i++)
+        if (b0 + i < nblocks) local += partials[b0 + i];
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(local, &total);
+    for (int i = 0; i < per; i++)
+        if (b0 + i < nblocks) {
+            const uint32_t t = partials[b0 + i];
+            partials[b0 + i] = run;
+            run += t;
+        }
+    if (threadIdx.x == 0) {
+        const bool over = total > (uint32_t)cap;
+        pair_count[0] = total > 0x7fffffffu ? 0x7fffffff : (int32_t)total;
+        pair_count[1] = over ? 1 : 0;
+    }
+}
+
+__global__ void scan_downsweep_kernel(int n, const uint32_t* __restrict__ in, const uint32_t* __restrict__ partials,
+                                      uint32_t* __restrict__ out) {
+    const int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;  // blocked arrangement
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        v[i] = (base + i < n) ? in[base + i] : 0;
+        s += v[i];
+    }
+    uint32_t run = block_exclusive_scan(s, nullptr) + partials[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        run += v[i];
+        if (base + i < n) out[base + i] = run;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// emit (tile, id) pairs in id order (reference duplicateWithKeysKernel,
+// cuda/forward.cu:28-47; the key keeps only the tile, the order is implied)
+// ---------------------------------------------------------------------------
+__global__ void duplicate_kernel(BinRule rule, int n, const float* __restrict__ rec,
+                                 const uint32_t* __restrict__ tiles_touched, const uint32_t* __restrict__ offsets,
+                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int cap) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t cnt = tiles_touched[g];
+    if (cnt == 0) return;
+    uint32_t off = offsets[g] - cnt;
+    const float2 m = *reinterpret_cast<const float2*>(rec + (size_t)g * kRecordFloats);
+    for_each_list_tile(rule, m.x, m.y, g, [&](int tile) {
+        if (off < (uint32_t)cap) {
+            keys[off] = (uint32_t)tile;
+            vals[off] = (uint32_t)g;
+        }
+        off++;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// stable LSD radix sort, 8-bit digits, keys = tile ids
+// ---------------------------------------------------------------------------
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per CTA
+constexpr int kSortWarpSpan = 32 * kSortItems;        // 512 keys per warp
+
+__global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(const uint32_t* __restrict__ keys,
+                                                                    const int32_t* __restrict__ pair_count, int cap,
+                                                                    int shift, uint32_t* __restrict__ hist,
+                                                                    int sort_ctas) {
+    __shared__ uint32_t h[256];
+    const int n = min(pair_count[0], cap);
+    const int base = blockIdx.x * kSortTile;
+    if (base >= n) return;  // columns past the active range are never read
+    h[threadIdx.x] = 0;
+    __syncthreads();
+#pragma unroll 4
+    for (int i = 0; i < kSortItems; i++) {
+        const int idx = base + i * kSortThreads + threadIdx.x;
+        if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * sort_ctas + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of hist in digit-major order over the active CTA columns.
+__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t* __restrict__ hist,
+                                                         const int32_t* __restrict__ pair_count, int cap,
+                                                         int sort_ctas) {
+    const int n = min(pair_count[0], cap);
+    const int active = (n + kSortTile - 1) / kSortTile;
+    if (active == 0) return;
+    const int total = 256 * active;
+    const int per = (total + blockDim.x - 1) / blockDim.x;
+    const int e0 = threadIdx.x * per;
+    uint32_t local = 0;
+    for (int i = 0; i < per; i++) {
+        const int e = e0 + i;
+        if (e < total) local += hist[(e / active) * sort_ctas + (e % active)];
+    }
+    uint32_t run = block_exclusive_scan(local, nullptr);
+    for (int i = 0; i < per; i++) {
+        const int e = e0 + i;
+        if (e < total) {
+            uint32_t* p = &hist[(e / active) * sort_ctas + (e % active)];
+            const uint32_t t = *p;
+            *p = run;
+            run += t;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
+    uint32_t* __restrict__ vals_out, const int32_t* __restrict__ pair_count, int cap, int shift,
+    const uint32_t* __restrict__ hist, int sort_ctas) {
+    __shared__ uint32_t wc[kSortWarps][257];  // slot 256 absorbs invalid lanes
+    const int n = min(pair_count[0], cap);
+    const int base = blockIdx.x * kSortTile;
+    if (base >= n) return;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < kSortWarps * 257; i += kSortThreads) (&wc[0][0])[i] = 0;
+    __syncthreads();
+
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+    const int wbase = base + w * kSortWarpSpan;
+#pragma unroll
+    for (int i = 0; i < kSortItems; i++) {
+        const int idx = wbase + i * 32 + lane;
+        const bool valid = idx < n;
+        key[i] = valid ? keys_in[idx] : 0u;
+        val[i] = valid ? vals_in[idx] : 0u;
+        const uint32_t d = valid ? ((key[i] >> shift) & 255u) : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = wc[w][d];
+        rank[i] = before + __popc(peers & lt_mask);
+        __syncwarp();
+        if (lane == __ffs(peers) - 1) wc[w][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // exclusive scan over warps for each digit
+    {
+        const int d = threadIdx.x;  // 256 threads = 256 digits
+        uint32_t run = 0;
+#pragma unroll
+        for (int ww = 0; ww < kSortWarps; ww++) {
+            const uint32_t c = wc[ww][d];
+            wc[ww][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kSortItems; i++) {
+        const int idx = wbase + i * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (key[i] >> shift) & 255u;
+            const uint32_t pos = hist[d * sort_ctas + blockIdx.x] + wc[w][d] + rank[i];
+            keys_out[pos] = key[i];
+            vals_out[pos] = val[i];
+        }
+    }
+}
+
+__global__ void zero_ranges_kernel(int32_t* __restrict__ ranges, int num_tiles) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < num_tiles) reinterpret_cast<int2*>(ranges)[i] = make_int2(0, 0);
+}
+
+// reference identifyTileRangesKernel (cuda/forward.cu:49-60)
+__global__ void ranges_kernel(const uint32_t* __restrict__ keys, const int32_t* __restrict__ pair_count, int cap,
+                              int32_t* __restrict__ ranges) {
+    const int n = min(pair_count[0], cap);
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const uint32_t tile = keys[idx];
+    if (idx == 0) {
+        ranges[2 * tile] = 0;
+    } else {
+        const uint32_t prev = keys[idx - 1];
+        if (prev != tile) {
+            ranges[2 * prev + 1] = idx;
+            ranges[2 * tile] = idx;
+        }
+    }
+    if (idx == n - 1) ranges[2 * tile + 1] = n;
+}
+
+BinWorkspace carve_bin_workspace(Carver& cv, int n, int cap) {
+    BinWorkspace ws;
+    ws.n = n;
+    ws.cap = cap;
+    ws.sort_ctas = (int)ceil_div((size_t)(cap > 0 ? cap : 1), kSortTile);
+    const int nscan = (int)ceil_div((size_t)(n > 0 ? n : 1), kScanBlock);
+    ws.tiles_touched = cv.take<uint32_t>(n > 0 ? n : 1);
+    ws.offsets = cv.take<uint32_t>(n > 0 ? n : 1);
+    ws.scan_partials = cv.take<uint32_t>(nscan);
+    ws.keys_a = cv.take<uint32_t>(cap > 0 ? cap : 1);
+    ws.keys_b = cv.take<uint32_t>(cap > 0 ? cap : 1);
+    ws.vals_a = cv.take<uint32_t>(cap > 0 ? cap : 1);
+    ws.vals_b = cv.take<uint32_t>(cap > 0 ? cap : 1);
+    ws.hist = cv.take<uint32_t>((size_t)256 * ws.sort_ctas);
+    return ws;
+}
+
+void launch_binning(const BinRule& rule, const float* records, const BinWorkspace& ws, int32_t* point_list,
+                    int32_t* ranges, int32_t* pair_count, cudaStream_t stream) {
+    const int num_lists = bin_rule_lists(rule);
+    const int n = ws.n;
+    zero_ranges_kernel<<<ceil_div(num_lists, 256), 256, 0, stream>>>(ranges, num_lists);
+    if (n <= 0) {
+        cudaMemsetAsync(pair_count, 0, 2 * sizeof(int32_t), stream);
+        return;
+    }
+    const int nscan = (int)ceil_div(n, kScanBlock);
+    scan_reduce_kernel<<<nscan, kScanThreads, 0, stream>>>(n, ws.tiles_touched, ws.scan_partials);
+    scan_partials_kernel<<<1, 1024, 0, stream>>>(nscan, ws.scan_partials, ws.cap, pair_count);
+    scan_downsweep_kernel<<<nscan, kScanThreads, 0, stream>>>(n, ws.tiles_touched, ws.scan_partials, ws.offsets);
+    if (ws.cap <= 0) return;
+    duplicate_kernel<<<ceil_div(n, 256), 256, 0, stream>>>(rule, n, records, ws.tiles_touched, ws.offsets,
+                                                           ws.keys_a, ws.vals_a, ws.cap);
+    int bits = 0;
+    while ((1 << bits) < num_lists) bits++;
+    const int passes = bits <= 8 ? 1 : (bits + 7) / 8;
+    const uint32_t* kin = ws.keys_a;
+    const uint32_t* vin = ws.vals_a;
+    for (int p = 0; p < passes; p++) {
+        uint32_t* kout = (p % 2 == 0) ? ws.keys_b : ws.keys_a;
+        uint32_t* vout = (p == passes - 1) ? reinterpret_cast<uint32_t*>(point_list)
+                                           : ((p % 2 == 0) ? ws.vals_b : ws.vals_a);
+        sort_upsweep_kernel<<<ws.sort_ctas, kSortThreads, 0, stream>>>(kin, pair_count, ws.cap, 8 * p, ws.hist,
+                                                                        ws.sort_ctas);
+        sort_scan_kernel<<<1, 1024, 0, stream>>>(ws.hist, pair_count, ws.cap, ws.sort_ctas);
+        sort_downsweep_kernel<<<ws.sort_ctas, kSortThreads, 0, stream>>>(kin, vin, kout, vout, pair_count, ws.cap,
+                                                                          8 * p, ws.hist, ws.sort_ctas);
+        kin = kout;
+        vin = vout;
+    }
+    ranges_kernel<<<ceil_div(ws.cap, 256), 256, 0, stream>>>(kin, pair_count, ws.cap, ranges);
+}
+
+// Index of the list a 16-px splat tile reads.
+__device__ __forceinline__ int list_of_tile(const BinRule& R, int tx, int ty) {
+    if (R.list_tile == kTile) return ty * R.lgx + tx;
+    if (R.list_tile == 64) return (ty >> 2) * R.lgx + (tx >> 2);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// splat forward: one CTA per 16x16 tile, one pixel per thread, each warp an
+// 8x4 pixel block; Gaussian batches of 256 records staged in shared memory.
+// ---------------------------------------------------------------------------
+template <int C>
+__global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
+    BinRule rule, const int32_t* __restrict__ ranges, const int32_t* __restrict__ point_list,
+    const float4* __restrict__ rec, const float* __restrict__ k, float dxy2, float2* __restrict__ out, int W, int H,
+    int gx) {
+    constexpr int NV = (8 + 2 * C + 3) / 4;  // float4 words used per record
+    __shared__ float4 s_rec[kTilePixels][NV];
+    const int tile = blockIdx.x;
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+    const int px = (tile % gx) * kTile + (w & 1) * 8 + (lane & 7);
+    const int py = (tile / gx) * kTile + (w >> 1) * 4 + (lane >> 3);
+    const float fx = (float)px, fy = (float)py;
+    const int2 range = reinterpret_cast<const int2*>(ranges)[list_of_tile(rule, tile % gx, tile / gx)];
+
+    float kc[C], acc_r[C], acc_i[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        kc[c] = k[c];
+        acc_r[c] = 0.0f;
+        acc_i[c] = 0.0f;
+    }
+
+    for (int b = range.x; b < range.y; b += kTilePixels) {
+        __syncthreads();
+        if (b + t < range.y) {
+            const int g = point_list[b + t];
+#pragma unroll
+            for (int q = 0; q < NV; q++) s_rec[t][q] = __ldg(&rec[(size_t)g * 4 + q]);
+        }
+        __syncthreads();
+        const int cnt = min(kTilePixels, range.y - b);
+        for (int j = 0; j < cnt; j++) {
+            const float4 r0 = s_rec[j][0];  // mx my i00 i01
+            const float4 r1 = s_rec[j][1];  // i11 opac curv area
+            const float dx = r0.x - fx, dy = r0.y - fy;
+            const float mahal = dx * (r0.z * dx + r0.w * dy) + dy * (r0.w * dx + r1.x * dy);
+            if (!__any_sync(0xffffffffu, mahal < kMahalCut)) continue;
+            const float power = fmaxf(-0.5f * mahal, -50.0f);
+            const float alpha = r1.y * __expf(power);
+            const float base = 0.5f * r1.z * mahal * r1.w * dxy2;
+            const float4 r2 = s_rec[j][2];
+            float col[C], ph[C];
+            if (C == 1) {
+                col[0] = r2.x;
+                ph[0] = r2.y;
+            } else {
+                const float4 r3 = s_rec[j][NV - 1];
+                col[0] = r2.x;
+                col[C > 1 ? 1 : 0] = r2.y;
+                col[C > 2 ? 2 : 0] = r2.z;
+                ph[0] = r2.w;
+                ph[C > 1 ? 1 : 0] = r3.x;
+                ph[C > 2 ? 2 : 0] = r3.y;
+            }
+#pragma unroll
+            for (int c = 0; c < C; c++) {
+                float s, co;
+                sincos_reduced(ph[c] + kc[c] * base, &s, &co);
+                const float amp = col[c] * alpha;
+                acc_r[c] = fmaf(amp, co, acc_r[c]);
+                acc_i[c] = fmaf(amp, s, acc_i[c]);
+            }
+        }
+    }
+    if (px < W && py < H) {
+        const size_t pid = (size_t)py * W + px;
+#pragma unroll
+        for (int c = 0; c < C; c++) out[(size_t)c * H * W + pid] = make_float2(acc_r[c], acc_i[c]);
+    }
+}
+
+void launch_splat_forward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
+                          const float* records, const float* k, float dxy2, float2* out, cudaStream_t stream) {
+    const int width = rule.width, height = rule.height;
+    const int gx = (width + kTile - 1) / kTile, gy = (height + kTile - 1) / kTile;
+    const float4* rec = reinterpret_cast<const float4*>(records);
+    if (channels == 1)
+        splat_forward_kernel<1><<<gx * gy, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2, out,
+                                                                     width, height, gx);
+    else
+        splat_forward_kernel<3><<<gx * gy, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2, out,
+                                                                     width, height, gx);
+}
+
+// ---------------------------------------------------------------------------
+// splat adjoint: Gaussian-parallel. One CTA per tile; each thread owns one
+// Gaussian of the tile list and walks the tile's 256 pixels in lockstep with
+// its warp, so the per-pixel dL/dU reads are shared-memory broadcasts and the
+// per-Gaussian sums stay in registers: no cross-lane reduction, and one atomic
+// per parameter per (Gaussian, tile). The per-pixel terms are recomputed, not
+// stored (same formulas as cuda/backward.cu:101-147, including both paths of
+// dL/dmahal).
+// ---------------------------------------------------------------------------
+constexpr int kBwdThreads = 64;
+
+template <int C>
+__global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
+    BinRule rule, const int32_t* __restrict__ ranges, const int32_t* __restrict__ point_list,
+    const float4* __restrict__ rec, const float* __restrict__ k, float dxy2, const float2* __restrict__ grad, int W,
+    int H, int gx, SplatGrads out) {
+    __shared__ float2 s_g[kTilePixels][C];
+    const int tile = blockIdx.x;
+    const int2 range = reinterpret_cast<const int2*>(ranges)[list_of_tile(rule, tile % gx, tile / gx)];
+    if (range.y <= range.x) return;
+    const int tx0 = (tile % gx) * kTile, ty0 = (tile / gx) * kTile;
+    for (int p = threadIdx.x; p < kTilePixels; p += kBwdThreads) {
+        const int px = tx0 + (p & 15), py = ty0 + (p >> 4);
+        const bool inside = px < W && py < H;
+#pragma unroll
+        for (int c = 0; c < C; c++)
+            s_g[p][c] = inside ? grad[(size_t)c * H * W + (size_t)py * W + px] : make_float2(0.0f, 0.0f);
+    }
+    __syncthreads();
+    const int xmax = min(kTile, W - tx0), ymax = min(kTile, H - ty0);
+
+    float kc[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) kc[c] = k[c];
+
+    for (int b = range.x; b < range.y; b += kBwdThreads) {
+        const int i = b + threadIdx.x;
+        if (i >= range.y) break;
+        const int g = point_list[i];
+        const float4 r0 = __ldg(&rec[(size_t)g * 4 + 0]);
+        const float4 r1 = __ldg(&rec[(size_t)g * 4 + 1]);
+        const float4 r2 = __ldg(&rec[(size_t)g * 4 + 2]);
+        const float4 r3 = __ldg(&rec[(size_t)g * 4 + 3]);
+        const float mx = r0.x, my = r0.y, i00 = r0.z, i01 = r0.w, i11 = r1.x;
+        const float opac = r1.y, curv = r1.z, ar = r1.w;
+        float col[C], ph[C];
+        if (C == 1) {
+            col[0] = r2.x;
+            ph[0] = r2.y;
+        } else {
+            col[0] = r2.x;
+            col[C > 1 ? 1 : 0] = r2.y;
+            col[C > 2 ? 2 : 0] = r2.z;
+            ph[0] = r2.w;
+            ph[C > 1 ? 1 : 0] = r3.x;
+            ph[C > 2 ? 2 : 0] = r3.y;
+        }
+        const float kb = 0.5f * curv * ar * dxy2;  // dbase/dmahal
+
+        float dmx = 0.f, dmy = 0.f, d00 = 0.f, d01 = 0.f, d11 = 0.f, dop = 0.f, dcv = 0.f, dar = 0.f;
+        float dcol[C], dph[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            dcol[c] = 0.f;
+            dph[c] = 0.f;
+        }
+        for (int yy = 0; yy < ymax; yy++) {
+            const float dy = my - (float)(ty0 + yy);
+            for (int xx = 0; xx < xmax; xx++) {
+                const float dx = mx - (float)(tx0 + xx);
+                const float mahal = dx * (i00 * dx + i01 * dy) + dy * (i01 * dx + i11 * dy);
+                if (mahal >= kMahalCut) continue;
+                const float raw_power = -0.5f * mahal;
+                const float G = __expf(fmaxf(raw_power, -50.0f));
+                const float alpha = opac * G;
+                const float base = 0.5f * curv * mahal * ar * dxy2;
+                const int p = yy * kTile + xx;
+                float S_alpha = 0.f, S_base = 0.f;
+#pragma unroll
+                for (int c = 0; c < C; c++) {
+                    float s, co;
+                    sincos_reduced(ph[c] + kc[c] * base, &s, &co);
+                    const float2 gp = s_g[p][c];
+                    const float proj_c = gp.x * co + gp.y * s;
+                    const float proj_s = -gp.x * s + gp.y * co;
+                    const float aph = col[c] * alpha * proj_s;
+                    dcol[c] = fmaf(alpha, proj_c, dcol[c]);
+                    dph[c] += aph;
+                    S_alpha = fmaf(col[c], proj_c, S_alpha);
+                    S_base = fmaf(kc[c], aph, S_base);
+                }
+                const float dpow = (raw_power >= -50.0f) ? -0.5f : 0.0f;
+                const float dmahal = S_alpha * opac * G * dpow + S_base * kb;
+                dcv = fmaf(S_base, 0.5f * mahal * ar * dxy2, dcv);
+                dar = fmaf(S_base, 0.5f * curv * mahal * dxy2, dar);
+                d00 = fmaf(dmahal, dx * dx, d00);
+                d01 = fmaf(dmahal, 2.0f * dx * dy, d01);
+                d11 = fmaf(dmahal, dy * dy, d11);
+                dmx = fmaf(dmahal, 2.0f * (i00 * dx + i01 * dy), dmx);
+                dmy = fmaf(dmahal, 2.0f * (i11 * dy + i01 * dx), dmy);
+                dop = fmaf(S_alpha, G, dop);
+            }
+        }
+        if (dmx != 0.f) atomicAdd(&out.d_means[2 * g], dmx);
+        if (dmy != 0.f) atomicAdd(&out.d_means[2 * g + 1], dmy);
+        if (d00 != 0.f) atomicAdd(&out.d_inv[3 * g], d00);
+        if (d01 != 0.f) atomicAdd(&out.d_inv[3 * g + 1], d01);
+        if (d11 != 0.f) atomicAdd(&out.d_inv[3 * g + 2], d11);
+        if (dop != 0.f) atomicAdd(&out.d_op[g], dop);
+        if (dcv != 0.f) atomicAdd(&out.d_cv[g], dcv);
+        if (dar != 0.f) atomicAdd(&out.d_ar[g], dar);
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            if (dcol[c] != 0.f) atomicAdd(&out.d_col[g * C + c], dcol[c]);
+            if (dph[c] != 0.f) atomicAdd(&out.d_ph[g * C + c], dph[c]);
+        }
+    }
+}
+
+void launch_splat_backward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
+                           const float* records, const float* k, float dxy2, const float2* grad,
+                           const SplatGrads& out, cudaStream_t stream) {
+    const int width = rule.width, height = rule.height;
+    const int gx = (width + kTile - 1) / kTile, gy = (height + kTile - 1) / kTile;
+    const float4* rec = reinterpret_cast<const float4*>(records);
+    if (channels == 1)
+        splat_backward_kernel<1><<<gx * gy, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2, grad,
+                                                                      width, height, gx, out);
+    else
+        splat_backward_kernel<3><<<gx * gy, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2, grad,
+                                                                      width, height, gx, out);
+}
+
+}  // namespace cvqpg
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace cvqpg;
+
+extern "C" const char* cvqpg_status_string(int status) {
+    switch (status) {
+        case CVQPG_OK: return "ok";
+        case CVQPG_ERR_ARG: return "invalid argument";
+        case CVQPG_ERR_CHANNELS: return "qpf rasterizer supports 1 or 3 channels";
+        case CVQPG_ERR_WORKSPACE: return "workspace too small";
+        case CVQPG_ERR_CUDA: return "CUDA launch failed";
+        case CVQPG_ERR_UNSUPPORTED: return "unsupported size";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int cvqpg_version(void) { return 100; }
+
+static size_t render_ws_bytes(int n, int cap) {
+    Carver cv(nullptr, 0);
+    cv.take<float>((size_t)(n > 0 ? n : 1) * kRecordFloats);
+    carve_bin_workspace(cv, n, cap);
+    return cv.off + 256;
+}
+
+extern "C" int cvqpg_render_workspace_size(int n, int width, int height, int pair_capacity, size_t* bytes) {
+    if (n < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || !bytes) return CVQPG_ERR_ARG;
+    *bytes = render_ws_bytes(n, pair_capacity);
+    return CVQPG_OK;
+}
+
+extern "C" int cvqpg_render_num_lists(int cull_mode, int width, int height) {
+    if (cull_mode < 0 || cull_mode > 2 || width <= 0 || height <= 0) return -1;
+    BinRule r = make_bin_rule(cull_mode, width, height, nullptr, nullptr);
+    return bin_rule_lists(r);
+}
+
+extern "C" int cvqpg_render_forward_cull(const float* means_2d, const float* inv_cov, const float* colours,
+                                         const float* phase, const float* opacities, const float* curvature,
+                                         const float* area, int cull_mode, const int32_t* radii,
+                                         const float* radius3, const float* k, float dxy2, int n, int width,
+                                         int height, int channels, float* out_field, int32_t* point_list,
+                                         int pair_capacity, int32_t* ranges, int32_t* pair_count, void* workspace,
+                                         size_t workspace_bytes, void* stream_) {
+    if (channels != 1 && channels != 3) return CVQPG_ERR_CHANNELS;
+    if (n < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || cull_mode < 0 || cull_mode > 2)
+        return CVQPG_ERR_ARG;
+    if (!k || !out_field || !ranges || !pair_count) return CVQPG_ERR_ARG;
+    if (n > 0 && (!means_2d || !inv_cov || !colours || !phase || !opacities || !curvature || !area ||
+                  !workspace || (pair_capacity > 0 && !point_list)))
+        return CVQPG_ERR_ARG;
+    if (n > 0 && cull_mode == CVQPG_CULL_CUDA16_5SIGMA && !radii) return CVQPG_ERR_ARG;
+    if (n > 0 && cull_mode == CVQPG_CULL_TORCH64_3SIGMA && !radius3) return CVQPG_ERR_ARG;
+    if (workspace_bytes < render_ws_bytes(n, pair_capacity)) return CVQPG_ERR_WORKSPACE;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    Carver cv(workspace, workspace_bytes);
+    float* rec = cv.take<float>((size_t)(n > 0 ? n : 1) * kRecordFloats);
+    BinWorkspace ws = carve_bin_workspace(cv, n, pair_capacity);
+    BinRule rule = make_bin_rule(cull_mode, width, height, radii, radius3);
+    launch_pack_records(channels, n, means_2d, inv_cov, colours, phase, opacities, curvature, area, rec, stream);
+    launch_tile_count(rule, rec, n, ws.tiles_touched, stream);
+    launch_binning(rule, rec, ws, point_list, ranges, pair_count, stream);
+    launch_splat_forward(channels, rule, ranges, point_list, rec, k, dxy2, reinterpret_cast<float2*>(out_field),
+                         stream);
+    return launch_status();
+}
+
+extern "C" int cvqpg_render_forward(const float* means_2d, const float* inv_cov, const float* colours,
+                                    const float* phase, const float* opacities, const float* curvature,
+                                    const float* area, const int32_t* radii, const float* k, float dxy2, int n,
+                                    int width, int height, int channels, float* out_field, int32_t* point_list,
+                                    int pair_capacity, int32_t* ranges, int32_t* pair_count, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+    return cvqpg_render_forward_cull(means_2d, inv_cov, colours, phase, opacities, curvature, area,
+                                     CVQPG_CULL_CUDA16_5SIGMA, radii, nullptr, k, dxy2, n, width, height, channels,
+                                     out_field, point_list, pair_capacity, ranges, pair_count, workspace,
+                                     workspace_bytes, stream);
+}
+
+extern "C" int cvqpg_render_backward_workspace_size(int n, size_t* bytes) {
+    if (n < 0 || !bytes) return CVQPG_ERR_ARG;
+    *bytes = (size_t)(n > 0 ? n : 1) * kRecordFloats * sizeof(float) + 256;
+    return CVQPG_OK;
+}
+
+extern "C" int cvqpg_render_backward_cull(const float* grad_field, const float* means_2d, const float* inv_cov,
+                                          const float* colours, const float* phase, const float* opacities,
+                                          const float* curvature, const float* area, const float* k,
+                                          int cull_mode, const int32_t* point_list, const int32_t* ranges,
+                                          float dxy2, int n, int width, int height, int channels, float* d_means,
+                                          float* d_inv_cov, float* d_colours, float* d_phase, float* d_opacities,
+                                          float* d_curvature, float* d_area, void* workspace,
+                                          size_t workspace_bytes, void* stream_) {
+    if (channels != 1 && channels != 3) return CVQPG_ERR_CHANNELS;
+    if (n < 0 || width <= 0 || height <= 0 || cull_mode < 0 || cull_mode > 2) return CVQPG_ERR_ARG;
+    if (n == 0) return CVQPG_OK;
+    if (!grad_field || !means_2d || !inv_cov || !colours || !phase || !opacities || !curvature || !area || !k ||
+        !point_list || !ranges || !d_means || !d_inv_cov || !d_colours || !d_phase || !d_opacities ||
+        !d_curvature || !d_area || !workspace)
+        return CVQPG_ERR_ARG;
+    size_t need = 0;
+    cvqpg_render_backward_workspace_size(n, &need);
+    if (workspace_bytes < need) return CVQPG_ERR_WORKSPACE;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    Carver cv(workspace, workspace_bytes);
+    float* rec = cv.take<float>((size_t)n * kRecordFloats);
+    const int C = channels;
+    cudaMemsetAsync(d_means, 0, sizeof(float) * 2 * n, stream);
+    cudaMemsetAsync(d_inv_cov, 0, sizeof(float) * 3 * n, stream);
+    cudaMemsetAsync(d_colours, 0, sizeof(float) * C * n, stream);
+    cudaMemsetAsync(d_phase, 0, sizeof(float) * C * n, stream);
+    cudaMemsetAsync(d_opacities, 0, sizeof(float) * n, stream);
+    cudaMemsetAsync(d_curvature, 0, sizeof(float) * n, stream);
+    cudaMemsetAsync(d_area, 0, sizeof(float) * n, stream);
+    launch_pack_records(C, n, means_2d, inv_cov, colours, phase, opacities, curvature, area, rec, stream);
+    BinRule rule = make_bin_rule(cull_mode, width, height, nullptr, nullptr);
+    SplatGrads out{d_means, d_inv_cov, d_colours, d_phase, d_opacities, d_curvature, d_area};
+    launch_splat_backward(C, rule, ranges, point_list, rec, k, dxy2, reinterpret_cast<const float2*>(grad_field),
+                          out, stream);
+    return launch_status();
+}
+
+extern "C" int cvqpg_render_backward(const float* grad_field, const float* means_2d, const float* inv_cov,
+                                     const float* colours, const float* phase, const float* opacities,
+                                     const float* curvature, const float* area, const float* k,
+                                     const int32_t* point_list, const int32_t* ranges, float dxy2, int n, int width,
+                                     int height, int channels, float* d_means, float* d_inv_cov, float* d_colours,
+                                     float* d_phase, float* d_opacities, float* d_curvature, float* d_area,
+                                     void* workspace, size_t workspace_bytes, void* stream) {
+    return cvqpg_render_backward_cull(grad_field, means_2d, inv_cov, colours, phase, opacities, curvature, area, k,
+                                      CVQPG_CULL_CUDA16_5SIGMA, point_list, ranges, dxy2, n, width, height,
+                                      channels, d_means, d_inv_cov, d_colours, d_phase, d_opacities, d_curvature,
+                                      d_area, workspace, workspace_bytes, stream);
+}

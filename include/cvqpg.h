@@ -1,0 +1,139 @@
+/*
+ * cvqpg.h - C ABI of the B200 (sm_100a) CVQPG hologram-fitting kernels.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (passed as void*, a cudaStream_t; NULL = legacy default stream), enqueues its
+ * kernels on that stream and returns a status code (CVQPG_OK = 0). Nothing in
+ * this header allocates device memory: scratch space is a caller-provided
+ * workspace whose size is reported by the matching *_workspace_size query.
+ * No entry point synchronises the host, so every one of them can be recorded
+ * into a CUDA graph.
+ *
+ * Layouts (all little-endian, C-contiguous):
+ *   complex fields  float2 (re, im) interleaved = torch.complex64 storage
+ *   per-Gaussian    SoA rows exactly as the reference tensors ([N,2], [N,3], [N,C], [N])
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   cuda/raster.cu:30-105   qpf_render_forward   -> cvqpg_render_forward
+ *   cuda/raster.cu:107-143  qpf_render_backward  -> cvqpg_render_backward
+ *   cuda/qpf_rasterizer.h:30-57 (declarations of the two above)
+ */
+#ifndef CVQPG_H_
+#define CVQPG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CVQPG_API __attribute__((visibility("default")))
+#else
+#define CVQPG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define CVQPG_OK 0
+#define CVQPG_ERR_ARG 1        /* invalid argument (null pointer, bad size)          */
+#define CVQPG_ERR_CHANNELS 2   /* channel count not 1 or 3 (cuda/forward.cu:173)     */
+#define CVQPG_ERR_WORKSPACE 3  /* workspace smaller than the size query reported     */
+#define CVQPG_ERR_CUDA 4       /* a kernel launch failed (cudaGetLastError)          */
+#define CVQPG_ERR_UNSUPPORTED 5 /* size/shape outside what the kernels were built for */
+
+/* ---- culling rules (which Gaussians enter which tile list) --------------- */
+#define CVQPG_CULL_CUDA16_5SIGMA 0  /* reference CUDA renderer: 16-px tiles, int radius rect */
+#define CVQPG_CULL_TORCH64_3SIGMA 1 /* reference torch renderer: 64-px tiles, 3-sigma circle */
+#define CVQPG_CULL_NONE 2           /* every Gaussian at every pixel                          */
+
+/* Human-readable text of a status code. */
+CVQPG_API const char* cvqpg_status_string(int status);
+
+/* Library version as 10000*major + 100*minor + patch. */
+CVQPG_API int cvqpg_version(void);
+
+/* ---- drop-in rasterizer ---------------------------------------------------
+ *
+ * cvqpg_render_forward replaces qpf_render_forward (cuda/raster.cu:30-105,
+ * declared at cuda/qpf_rasterizer.h:30-41). Same inputs and meaning:
+ *   means_2d [N,2] pixel coords, inv_cov [N,3] (inv00, inv01, inv11),
+ *   colours [N,C], phase [N,C], opacities [N], curvature [N], area [N] = |sx*sy|,
+ *   radii [N] int32 culling radius in px, k [C] wavenumbers, dxy2 = pitch^2.
+ * Outputs:
+ *   out_field  [C,H,W] complex64, fully written (no pre-zeroing needed)
+ *   point_list [pair_capacity] int32, Gaussian ids sorted by (tile, id)
+ *   ranges     [T,2] int32, T = ceil(W/16)*ceil(H/16), [start,end) per tile
+ *   pair_count [2] int32 (device): [0] = pairs required (the reference's
+ *              total_pairs), [1] = 1 if that exceeded pair_capacity (then only
+ *              the first pair_capacity pairs were binned, the field is
+ *              incomplete and the caller must retry with a larger capacity)
+ * The tile lists are bit-identical to the reference's 64-bit (tile<<32 | id)
+ * CUB sort: the pairs are generated in id order and a stable LSD radix sort on
+ * the tile bits keeps that order inside each tile.
+ * Errors: CVQPG_ERR_CHANNELS for C not in {1,3} (cuda/forward.cu:173),
+ * CVQPG_ERR_ARG for null pointers / negative sizes (cuda/raster.cu:22-28).
+ */
+CVQPG_API int cvqpg_render_workspace_size(int n, int width, int height, int pair_capacity, size_t* bytes);
+
+CVQPG_API int cvqpg_render_forward(const float* means_2d, const float* inv_cov, const float* colours,
+                         const float* phase, const float* opacities, const float* curvature,
+                         const float* area, const int32_t* radii, const float* k, float dxy2,
+                         int n, int width, int height, int channels,
+                         float* out_field, int32_t* point_list, int pair_capacity, int32_t* ranges,
+                         int32_t* pair_count, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Number of tile lists (rows of `ranges`) a culling rule produces. */
+CVQPG_API int cvqpg_render_num_lists(int cull_mode, int width, int height);
+
+/* Forward with an explicit culling rule, so that each parity check compares
+ * like with like: CVQPG_CULL_CUDA16_5SIGMA uses `radii` (as
+ * cvqpg_render_forward), CVQPG_CULL_TORCH64_3SIGMA uses `radius3` = the
+ * torch renderer's float 3-sigma radius (model_2d_gaussian_rgb.py:400-403)
+ * and 64-px lists (model_2d_gaussian_rgb.py:311-314), CVQPG_CULL_NONE sums
+ * every Gaussian at every pixel (cuda/rasterizer.py:74-91). `ranges` has
+ * cvqpg_render_num_lists(cull_mode, W, H) rows.
+ */
+CVQPG_API int cvqpg_render_forward_cull(const float* means_2d, const float* inv_cov, const float* colours,
+                                        const float* phase, const float* opacities, const float* curvature,
+                                        const float* area, int cull_mode, const int32_t* radii,
+                                        const float* radius3, const float* k, float dxy2, int n, int width,
+                                        int height, int channels, float* out_field, int32_t* point_list,
+                                        int pair_capacity, int32_t* ranges, int32_t* pair_count,
+                                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* cvqpg_render_backward replaces qpf_render_backward (cuda/raster.cu:107-143,
+ * declared at cuda/qpf_rasterizer.h:43-57). grad_field is dL/d(field) as a
+ * complex64 [C,H,W] tensor (real part = dL/dRe, imaginary part = dL/dIm, the
+ * torch convention). point_list/ranges come from the forward.
+ * Outputs (overwritten, not accumulated): d_means [N,2], d_inv_cov [N,3],
+ * d_colours [N,C], d_phase [N,C], d_opacities [N], d_curvature [N], d_area [N].
+ * The workspace (size from cvqpg_render_backward_workspace_size) holds the
+ * packed per-Gaussian records.
+ */
+CVQPG_API int cvqpg_render_backward_workspace_size(int n, size_t* bytes);
+
+CVQPG_API int cvqpg_render_backward(const float* grad_field, const float* means_2d, const float* inv_cov,
+                          const float* colours, const float* phase, const float* opacities,
+                          const float* curvature, const float* area, const float* k,
+                          const int32_t* point_list, const int32_t* ranges, float dxy2,
+                          int n, int width, int height, int channels,
+                          float* d_means, float* d_inv_cov, float* d_colours, float* d_phase,
+                          float* d_opacities, float* d_curvature, float* d_area,
+                          void* workspace, size_t workspace_bytes, void* stream);
+
+/* Backward matching cvqpg_render_forward_cull (same cull_mode, lists, ranges). */
+CVQPG_API int cvqpg_render_backward_cull(const float* grad_field, const float* means_2d, const float* inv_cov,
+                                         const float* colours, const float* phase, const float* opacities,
+                                         const float* curvature, const float* area, const float* k,
+                                         int cull_mode, const int32_t* point_list, const int32_t* ranges,
+                                         float dxy2, int n, int width, int height, int channels,
+                                         float* d_means, float* d_inv_cov, float* d_colours, float* d_phase,
+                                         float* d_opacities, float* d_curvature, float* d_area,
+                                         void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVQPG_H_ */

@@ -1,0 +1,262 @@
+"""Generate the golden fixtures under tests/golden/ by running the reference.
+
+This script imports the reference CVQPG Python modules from REFERENCE_DIR
+(default /root/reference, the read-only checkout present on the build machine)
+and records their outputs on small seeded inputs. The fixtures pin the CPU
+oracle (oracle/) and the CUDA kernels to the reference's own behaviour.
+
+Reference pieces used (paths inside the reference project):
+  cuda/rasterizer.py:74-91     qpf_render_reference (uncut splat, float64 + autograd)
+  model_2d_gaussian_rgb.py     Gaussians2D activations/covariance, Scene2D torch tile renderer,
+  model_2d_gaussian_grayscale.py  soft_window_pad
+  utils/optimizer.py           Adan (loaded by path; utils/__init__ pulls uninstalled packages)
+  utils/propagator.py          propagator / multiplane_loss_odak, with the oracle's restatement of
+                               the odak functions installed as the `odak` module (odak 0.2.7 is not
+                               installed here, so that part stays unpinned)
+  utils/data_utils.py          GaussianLoss (SSIM) with the oracle's restatement of pytorch_msssim
+                               installed as `pytorch_msssim` (1.0.0 not installed: unpinned)
+
+Run:  python tests/golden/make_golden.py [--only NAME ...]
+"""
+import argparse
+import importlib.util
+import math
+import os
+import sys
+import types
+from argparse import Namespace
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REFERENCE_DIR = os.environ.get("CVQPG_REFERENCE_DIR", "/root/reference")
+sys.path.insert(0, REPO)
+
+
+def load_by_path(name, path):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def ref(path):
+    return os.path.join(REFERENCE_DIR, path)
+
+
+def install_third_party_restatements():
+    """Install the oracle's restatements of odak / pytorch_msssim under their import names."""
+    from oracle import odak_restated, ssim as ssim_mod
+    odak = types.ModuleType("odak")
+    odak.pi = math.pi
+    learn = types.ModuleType("odak.learn")
+    wave = types.ModuleType("odak.learn.wave")
+    tools = types.ModuleType("odak.learn.tools")
+    for n in ("get_propagation_kernel", "generate_complex_field", "calculate_amplitude", "calculate_phase"):
+        setattr(wave, n, getattr(odak_restated, n))
+    for n in ("zero_pad", "crop_center", "generate_2d_gaussian"):
+        setattr(tools, n, getattr(odak_restated, n))
+    learn.wave, learn.tools = wave, tools
+    odak.learn = learn
+    sys.modules.update({"odak": odak, "odak.learn": learn, "odak.learn.wave": wave, "odak.learn.tools": tools})
+    ms = types.ModuleType("pytorch_msssim")
+    ms.SSIM = ssim_mod.SSIMModule
+    sys.modules["pytorch_msssim"] = ms
+
+
+# ---------------------------------------------------------------------------
+# seeded synthetic Gaussians (activated parameters)
+# ---------------------------------------------------------------------------
+WAVELENGTHS = [639e-9, 515e-9, 473e-9]
+PITCH = 3.74e-6
+
+
+def activated_params(rng, n, W, H, C, margin=3.0):
+    means = np.stack([rng.uniform(-margin, W + margin, n), rng.uniform(-margin, H + margin, n)], 1).astype(np.float32)
+    s = (np.exp(rng.normal(math.log(2.0), 0.3, (n, 2))) + 0.1).astype(np.float32)
+    rot = rng.uniform(0, math.pi, n).astype(np.float32)
+    t = torch.from_numpy
+    c, si = torch.cos(t(rot)), torch.sin(t(rot))
+    sx2, sy2 = t(s[:, 0]) ** 2, t(s[:, 1]) ** 2
+    cov00 = sx2 * c * c + sy2 * si * si + 0.1
+    cov01 = (sx2 - sy2) * c * si
+    cov11 = sx2 * si * si + sy2 * c * c + 0.1
+    det = (cov00 * cov11 - cov01 * cov01).clamp(min=1e-10)
+    inv = torch.stack([cov11 / det, -cov01 / det, cov00 / det], -1).numpy().astype(np.float32)
+    colours = rng.uniform(0, 1, (n, C)).astype(np.float32)
+    phase = rng.uniform(0, 2 * math.pi, (n, C)).astype(np.float32)
+    opac = rng.uniform(0.2, 0.9, n).astype(np.float32)
+    lam_min = min(WAVELENGTHS[:C]) if C == 3 else WAVELENGTHS[0]
+    cmax = 0.9 * lam_min / (6.0 * s.max(1) * PITCH ** 2)
+    curv = (cmax * np.tanh(rng.normal(0, 1, n))).astype(np.float32)
+    area = np.abs(s[:, 0] * s[:, 1]).astype(np.float32)
+    wl = WAVELENGTHS if C == 3 else WAVELENGTHS[:1]
+    k = (2 * np.pi / torch.tensor(wl, dtype=torch.float32)).numpy().astype(np.float32)
+    dxy2 = np.float32(PITCH ** 2)
+    cov = np.stack([cov00.numpy(), cov01.numpy(), cov11.numpy()], 1).astype(np.float32)
+    return dict(means=means, inv_cov=inv, colours=colours, phase=phase, opac=opac, curv=curv, area=area, k=k,
+                dxy2=dxy2, cov=cov)
+
+
+# ---------------------------------------------------------------------------
+# fixtures
+# ---------------------------------------------------------------------------
+def golden_splat(C, name, seed, n=200, W=50, H=40):
+    rasterizer = load_by_path("ref_cuda_rasterizer", ref("cuda/rasterizer.py"))
+    rng = np.random.default_rng(seed)
+    p = activated_params(rng, n, W, H, C)
+    T = lambda a: torch.from_numpy(np.asarray(a, dtype=np.float64)).requires_grad_(True)
+    ins = [T(p[k]) for k in ("means", "inv_cov", "colours", "phase", "opac", "curv", "area")]
+    out = rasterizer.qpf_render_reference(*ins, torch.from_numpy(p["k"].astype(np.float64)), float(p["dxy2"]), W, H)
+    gw = rng.normal(0, 1, (C, H, W)) + 1j * rng.normal(0, 1, (C, H, W))
+    loss = (out.real * torch.from_numpy(gw.real)).sum() + (out.imag * torch.from_numpy(gw.imag)).sum()
+    loss.backward()
+    grads = {f"d_{k}": t.grad.numpy() for k, t in zip(("means", "inv_cov", "colours", "phase", "opac", "curv", "area"),
+                                                       ins)}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), W=W, H=H, grad_field=gw, out=out.detach().numpy(),
+                        **p, **grads)
+
+
+def _args_prop(C, pad_size, renderer="torch"):
+    wl = WAVELENGTHS if C == 3 else WAVELENGTHS[:1]
+    return Namespace(wavelengths=list(wl), pixel_pitch=PITCH, pad_size=list(pad_size), tile_size=64, gauss_batch=1024,
+                     phase_iso=False, grad_ckpt=False, renderer=renderer, curv_nyquist=0.9)
+
+
+def raw_params(rng, n, W, H, C, curv_scale=1.0):
+    """Raw (pre-activation) parameters in the Gaussians2D layout (model_2d_gaussian_rgb.py:18-26)."""
+    mx = rng.uniform(0, W, n) / W * 2 - 1
+    my = rng.uniform(0, H, n) / H * 2 - 1
+    means = np.arctanh(np.clip(np.stack([mx, my], 1), -0.999, 0.999)).astype(np.float32)
+    scales = np.log(np.exp(rng.normal(math.log(2.0), 0.3, (n, 2)))).astype(np.float32)
+    rot = rng.uniform(-math.pi, math.pi, n).astype(np.float32)
+    colours = rng.uniform(0, 1, (n, C)).astype(np.float32)
+    phase = rng.uniform(-1.0, 7.5, (n, C)).astype(np.float32)   # exercises the mod-2pi wrap
+    opac = rng.normal(-0.5, 1.0, n).astype(np.float32)
+    curv = (curv_scale * rng.normal(0, 0.5, n)).astype(np.float32)
+    return dict(means_2d=means, pre_act_scales=scales, pre_act_rotation=rot, colours=colours,
+                pre_act_phase=phase, pre_act_opacities=opac, curvature=curv)
+
+
+RAW_KEYS = ("means_2d", "pre_act_scales", "pre_act_rotation", "colours", "pre_act_phase", "pre_act_opacities",
+            "curvature")
+
+
+def _make_gaussians(model, raw, W, H, C, args_prop, curv_mode):
+    g = model.Gaussians2D(num_points=raw["means_2d"].shape[0], img_size=(W, H), device="cpu", args_prop=args_prop)
+    for k in RAW_KEYS:
+        getattr(g, k).data.copy_(torch.from_numpy(raw[k]))
+    g.curv_mode = curv_mode
+    model.make_trainable_2d(g)
+    return g
+
+
+def golden_preprocess(C, name, seed, n=300, W=96, H=80):
+    model = load_by_path(f"ref_model_{C}", ref("model_2d_gaussian_rgb.py" if C == 3 else
+                                              "model_2d_gaussian_grayscale.py"))
+    rng = np.random.default_rng(seed)
+    raw = raw_params(rng, n, W, H, C)
+    raw["pre_act_scales"][:5, 0] = raw["pre_act_scales"][:5, 1]  # ties in max(scales)
+    out = {}
+    for mode in ("scale_aware", "constant", "off"):
+        g = _make_gaussians(model, raw, W, H, C, _args_prop(C, (H + 32, W + 32)), mode)
+        scales, rotation, phase, opac, means, curv = g.apply_activations()
+        c00, c01, c11 = g.compute_2d_covariance_elements(scales, rotation)
+        i00, i01, i11 = g.invert_cov_2D(c00, c01, c11)
+        area = (scales[:, 0] * scales[:, 1]).abs()
+        with torch.no_grad():
+            mid = 0.5 * (c00 + c11)
+            disc = torch.sqrt(((c00 - c11) * 0.5) ** 2 + c01 ** 2)
+            radii = (5.0 * torch.sqrt(mid + disc)).ceil().to(torch.int32)
+            radius3 = 3.0 * torch.sqrt(mid + disc)
+        outs = dict(means=means, inv_cov=torch.stack([i00, i01, i11], -1), phase=phase, opac=opac, curv=curv,
+                    area=area, cov=torch.stack([c00, c01, c11], -1))
+        rng2 = np.random.default_rng(seed + 1)
+        wts = {k: torch.from_numpy(rng2.normal(0, 1, v.shape).astype(np.float32)) for k, v in outs.items()
+               if k != "cov"}
+        loss = sum((v * wts[k]).sum() for k, v in outs.items() if k != "cov")
+        loss.backward()
+        for k, v in outs.items():
+            out[f"{mode}__{k}"] = v.detach().numpy()
+        for k, v in wts.items():
+            out[f"{mode}__w_{k}"] = v.numpy()
+        out[f"{mode}__radii"] = radii.numpy()
+        out[f"{mode}__radius3"] = radius3.numpy()
+        for k in RAW_KEYS:
+            gr = getattr(g, k).grad
+            out[f"{mode}__grad_{k}"] = np.zeros(raw[k].shape, np.float32) if gr is None else gr.numpy()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), W=W, H=H, C=C, **raw, **out)
+
+
+def golden_torch_renderer(C, name, seed, n=400, W=160, H=112, pad=(176, 224)):
+    """The reference torch tile renderer (3-sigma 64-px culling) + soft_window_pad, with gradients."""
+    model = load_by_path(f"ref_model_{C}", ref("model_2d_gaussian_rgb.py" if C == 3 else
+                                              "model_2d_gaussian_grayscale.py"))
+    rng = np.random.default_rng(seed)
+    raw = raw_params(rng, n, W, H, C, curv_scale=2.0)
+    ap = _args_prop(C, pad)
+    g = _make_gaussians(model, raw, W, H, C, ap, "scale_aware")
+    with torch.no_grad():
+        scales, rotation, phase, opac, means, curv = g.apply_activations()
+        c00, c01, c11 = g.compute_2d_covariance_elements(scales, rotation)
+        i00, i01, i11 = g.invert_cov_2D(c00, c01, c11)
+        mid = 0.5 * (c00 + c11)
+        disc = torch.sqrt(((c00 - c11) * 0.5) ** 2 + c01 ** 2)
+        act = dict(act_means=means.numpy(), act_inv_cov=torch.stack([i00, i01, i11], -1).numpy(),
+                   act_phase=phase.numpy(), act_opac=opac.numpy(), act_curv=curv.numpy(),
+                   act_area=(scales[:, 0] * scales[:, 1]).abs().numpy(), act_radius3=(3.0 * torch.sqrt(mid + disc)).numpy(),
+                   act_radii=(5.0 * torch.sqrt(mid + disc)).ceil().to(torch.int32).numpy(),
+                   act_k=(2 * np.pi / torch.tensor(ap.wavelengths, dtype=torch.float32)).numpy(),
+                   act_dxy2=np.float32(ap.pixel_pitch ** 2))
+    g.invalidate_cache()
+    scene = model.Scene2D(g, ap)
+    saved = model.soft_window_pad
+    model.soft_window_pad = lambda h, p: h
+    try:
+        field = scene.render((W, H))
+    finally:
+        model.soft_window_pad = saved
+    padded = saved(field, ap.pad_size)
+    gw = torch.from_numpy((rng.normal(0, 1, padded.shape) + 1j * rng.normal(0, 1, padded.shape)).astype(np.complex64))
+    loss = (padded.real * gw.real).sum() + (padded.imag * gw.imag).sum()
+    loss.backward()
+    grads = {f"grad_{k}": getattr(g, k).grad.numpy() for k in RAW_KEYS}
+    # field-level gradient of the same loss through the pad (for the pad adjoint)
+    f2 = field.detach().clone().requires_grad_(True)
+    l2 = (saved(f2, ap.pad_size).real * gw.real).sum() + (saved(f2, ap.pad_size).imag * gw.imag).sum()
+    l2.backward()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), W=W, H=H, C=C, pad=np.array(pad), **raw,
+                        field=field.detach().numpy(), padded=padded.detach().numpy(), grad_padded=gw.numpy(),
+                        grad_field=f2.grad.numpy(), **grads, **act)
+
+
+GOLDENS = {
+    "splat_rgb": lambda: golden_splat(3, "splat_rgb", 11),
+    "splat_gray": lambda: golden_splat(1, "splat_gray", 12),
+    "preprocess_rgb": lambda: golden_preprocess(3, "preprocess_rgb", 21),
+    "preprocess_gray": lambda: golden_preprocess(1, "preprocess_gray", 22),
+    "torch_renderer_rgb": lambda: golden_torch_renderer(3, "torch_renderer_rgb", 31),
+    "torch_renderer_gray": lambda: golden_torch_renderer(1, "torch_renderer_gray", 32),
+}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*", default=None)
+    a = ap.parse_args()
+    if not os.path.isdir(REFERENCE_DIR):
+        raise SystemExit(f"reference checkout not found at {REFERENCE_DIR}")
+    torch.set_num_threads(8)
+    install_third_party_restatements()
+    for name, fn in GOLDENS.items():
+        if a.only and name not in a.only:
+            continue
+        print("golden:", name, flush=True)
+        fn()
+
+
+if __name__ == "__main__":
+    main()
