@@ -35,6 +35,11 @@ _SIGNATURES = {
                               _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
     "cvqpg_render_backward_cull": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _f, _i, _i, _i, _i,
                                    _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
+    "cvqpg_blasm_tables_size": [_p, _psz],
+    "cvqpg_blasm_setup": [_p, _p, _sz],
+    "cvqpg_blasm_workspace_size": [_p, _psz],
+    "cvqpg_blasm_forward": [_p, _p, _sz, _p, _p, _p, _sz, _p],
+    "cvqpg_blasm_backward": [_p, _p, _sz, _p, _p, _p, _p, _sz, _p],
 }
 _RESTYPES = {"cvqpg_status_string": ctypes.c_char_p}
 

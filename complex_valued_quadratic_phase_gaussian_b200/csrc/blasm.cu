@@ -1,0 +1,629 @@
+// Band-limited angular-spectrum propagation of the CVQPG hologram to every
+// (plane, wavelength) in three pruned FFT passes, and its adjoint.
+//
+// Reference chain replaced (paths inside the reference project):
+//   model_2d_gaussian_rgb.py:186-241   soft_window_pad (replicate guard band, Tukey taper)
+//   train_2d_gaussian_rgb.py:89-95     phase = angle(U) mod 2pi, amplitude = clamp(|U|, 0, 1)
+//   utils/propagator.py:248-290        per (plane, channel): zero_pad x2, fft2, fftshift,
+//                                      aperture, transfer function, ifftshift, ifft2, crop
+//   utils/propagator.py:41-64          custom()
+//   utils/propagator.py:202-222        transfer-function cache (odak BLASM kernel)
+//   train_2d_gaussian_rgb.py:193       crop_center to the image
+//
+// Grid facts used for pruning (all sizes even): the padded field occupies
+// rows [NH/2 - pH/2, NH/2 + pH/2) of the 2x grid, and the kept output rows are
+// [NH/2 - out_h/2, NH/2 + out_h/2); for even n, fftshift and ifftshift are the
+// same half-length rotation, so the shifted multiply equals an unshifted one
+// by M[(k + N/2) mod N].
+#include <math.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "blasm.cuh"
+
+namespace cvqpg {
+
+// ---------------------------------------------------------------------------
+// host: FFT plans
+// ---------------------------------------------------------------------------
+bool make_fft_plan(int n, FftPlan* plan) {
+    plan->n = n;
+    plan->npass = 0;
+    plan->code = 0;
+    plan->tw = nullptr;
+    int m = n;
+    auto push = [&](int r) {
+        if (plan->npass >= kMaxPasses) return false;
+        plan->code |= (unsigned long long)r << (5 * plan->npass);
+        plan->npass++;
+        return true;
+    };
+    while (m % 16 == 0)
+        if (!push(16)) return false; else m /= 16;
+    if (m % 8 == 0) { if (!push(8)) return false; m /= 8; }
+    if (m % 4 == 0) { if (!push(4)) return false; m /= 4; }
+    if (m % 2 == 0) { if (!push(2)) return false; m /= 2; }
+    const int odd[] = {3, 5, 7, 11, 13, 17};
+    for (int r : odd)
+        while (m % r == 0) {
+            if (!push(r)) return false;
+            m /= r;
+        }
+    return m == 1;
+}
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+// Transfer function times 1/(NH*NW) at natural FFT index (ky, kx).
+__device__ __forceinline__ float2 transfer(const BlasmDev& d, const PCParam& pp, int c, int ky, int kx) {
+    int j = ky + (d.NH >> 1);
+    if (j >= d.NH) j -= d.NH;
+    int i = kx + (d.NW >> 1);
+    if (i >= d.NW) i -= d.NW;
+    if (j < pp.j0 || j >= pp.j1) return make_float2(0.f, 0.f);
+    const int2 ap = d.aperture[j];
+    const int lo = max(pp.i0, ap.x), hi = min(pp.i1, ap.y);
+    if (i < lo || i >= hi) return make_float2(0.f, 0.f);
+    const float u = __ldg(&d.a_row[c * d.NH + j]) + __ldg(&d.b_col[c * d.NW + i]);
+    if (!(u < 1.0f)) return make_float2(0.f, 0.f);  // evanescent: excluded
+    // 2 pi z sqrt(1/lambda^2 - f^2) = theta0 + K (sqrt(1-u) - 1),  sqrt(1-u) - 1 = -u / (1 + sqrt(1-u))
+    const float th = pp.theta0 - pp.K * u / (1.0f + sqrtf(1.0f - u));
+    float sn, cs;
+    sincos_reduced(th, &sn, &cs);
+    return make_float2(cs * d.scale, sn * d.scale);
+}
+
+// amplitude clamp to 1 keeping the phase (reference: generate_complex_field(clamp(|U|,0,1), angle(U)))
+__device__ __forceinline__ float2 clamp_amplitude(float2 u) {
+    const float r2 = u.x * u.x + u.y * u.y;
+    if (r2 <= 1.0f) return u;
+    const float inv = rsqrtf(r2);
+    return make_float2(u.x * inv, u.y * inv);
+}
+
+// adjoint of clamp_amplitude at u for the incoming gradient g (torch convention)
+__device__ __forceinline__ float2 clamp_amplitude_adjoint(float2 u, float2 g) {
+    const float r2 = u.x * u.x + u.y * u.y;
+    if (r2 == 0.0f) return make_float2(0.f, 0.f);
+    if (r2 <= 1.0f) return g;
+    const float r = sqrtf(r2);
+    const float c = u.x / r, s = u.y / r;
+    const float gphi = -g.x * s + g.y * c;
+    return make_float2(-gphi * u.y / r2, gphi * u.x / r2);
+}
+
+// ---------------------------------------------------------------------------
+// forward kernels
+// ---------------------------------------------------------------------------
+constexpr int kRowThreads = 256;
+constexpr int kColThreads = 512;
+
+__host__ __device__ constexpr int ilog2c(int g) { return g >= 4 ? 2 : (g >= 2 ? 1 : 0); }
+
+// K1: one padded row per CTA. The first FFT pass reads the splat field directly
+// (replicate guard band, Tukey window, amplitude clamp on the fly); output in
+// the tiled layout [C][NW/G][pH][G] that the column pass reads contiguously.
+__global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_kernel(BlasmDev d, const float2* __restrict__ in,
+                                                                     float2* __restrict__ A) {
+    extern __shared__ float2 sm[];
+    const int ld = fft_ld(d.NW);
+    float2* b0 = sm;
+    float2* b1 = sm + ld;
+    const int c = blockIdx.x / d.pH, y = blockIdx.x - c * d.pH;
+    const int x0 = (d.NW >> 1) - (d.pW >> 1);
+    const int pW = d.pW;
+    float2* res;
+    if (d.input_mode == 0) {
+        const int yy = min(max(y - d.pad_h, 0), d.H - 1);
+        const float wyv = __ldg(&d.wy[y]);
+        const float2* src = in + ((size_t)c * d.H + yy) * d.W;
+        const float* wx = d.wx;
+        const int pad_w = d.pad_w, W = d.W;
+        res = fft_run(
+            [=](int, int e) {
+                const int x = e - x0;
+                if (x < 0 || x >= pW) return make_float2(0.f, 0.f);
+                const int xx = min(max(x - pad_w, 0), W - 1);
+                const float w = wyv * __ldg(&wx[x]);
+                const float2 u = __ldg(&src[xx]);
+                return clamp_amplitude(make_float2(u.x * w, u.y * w));
+            },
+            b0, b1, ld, 0, d.row, false);
+    } else {
+        const float2* src = in + ((size_t)c * d.pH + y) * d.pW;
+        res = fft_run(
+            [=](int, int e) {
+                const int x = e - x0;
+                return (x < 0 || x >= pW) ? make_float2(0.f, 0.f) : __ldg(&src[x]);
+            },
+            b0, b1, ld, 0, d.row, false);
+    }
+    const int G = d.G, ngroups = d.NW / G;
+    for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) {
+        const int gi = kx / G, g = kx - gi * G;
+        A[(((size_t)c * ngroups + gi) * d.pH + y) * G + g] = res[fft_pad(kx)];
+    }
+}
+
+// K2: G columns per CTA: forward FFT (length NH) once, then per plane an
+// inverse FFT whose first pass multiplies by the transfer function on load;
+// keep out_h rows -> B [P*C][out_h][NW].
+template <int G>
+__global__ void __launch_bounds__(kColThreads, 1) blasm_cols_fwd_kernel(BlasmDev d, const float2* __restrict__ A,
+                                                                        float2* __restrict__ B) {
+    extern __shared__ float2 sm[];
+    constexpr int TS = ilog2c(G);
+    const int ld = fft_ld(d.NH);
+    float2* buf[3] = {sm, sm + G * ld, sm + 2 * G * ld};
+    const int ngroups = d.NW / G;
+    const int c = blockIdx.x / ngroups, gi = blockIdx.x - c * ngroups;
+    const int kx0 = gi * G;
+    const int y0 = (d.NH >> 1) - (d.pH >> 1);
+    const int pH = d.pH;
+    const float2* src = A + ((size_t)c * ngroups + gi) * pH * G;
+    float2* spec = fft_run(
+        [=](int t, int e) {
+            const int y = e - y0;
+            return (y < 0 || y >= pH) ? make_float2(0.f, 0.f) : __ldg(&src[y * G + t]);
+        },
+        buf[0], buf[1], ld, TS, d.col, false);
+    float2* w0 = spec == buf[0] ? buf[1] : buf[0];
+    float2* w1 = buf[2];
+    const int row0 = (d.NH >> 1) - (d.out_h >> 1);
+    for (int p = 0; p < d.P; p++) {
+        const int pc = p * d.C + c;
+        const PCParam pp = d.pcp[pc];
+        const float2* sp = spec;
+        float2* res = fft_run(
+            [=](int t, int e) { return cmul(sp[t * ld + fft_pad(e)], transfer(d, pp, c, e, kx0 + t)); }, w0, w1, ld,
+            TS, d.col, true);
+        float2* dst = B + (size_t)pc * d.out_h * d.NW + kx0;
+        for (int e = threadIdx.x; e < d.out_h * G; e += blockDim.x) {
+            const int y = e >> TS, g = e & (G - 1);
+            dst[(size_t)y * d.NW + g] = res[g * ld + fft_pad(row0 + y)];
+        }
+        __syncthreads();
+    }
+}
+
+// K3: inverse FFT of a kept row (first pass reads global), keep out_w columns
+// -> V [P*C][out_h][out_w]
+__global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_kernel(BlasmDev d, const float2* __restrict__ B,
+                                                                     float2* __restrict__ V) {
+    extern __shared__ float2 sm[];
+    const int ld = fft_ld(d.NW);
+    const size_t row = blockIdx.x;  // pc * out_h + y
+    const float2* src = B + row * d.NW;
+    float2* res = fft_run([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, 0, d.row, true);
+    const int col0 = (d.NW >> 1) - (d.out_w >> 1);
+    float2* dst = V + row * d.out_w;
+    for (int x = threadIdx.x; x < d.out_w; x += blockDim.x) dst[x] = res[fft_pad(col0 + x)];
+}
+
+// ---------------------------------------------------------------------------
+// adjoint kernels
+// ---------------------------------------------------------------------------
+// K3b: gradient row embedded at the out_w centred columns -> forward FFT ->
+// tiled [P*C][NW/G][out_h][G]
+__global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_adj_kernel(BlasmDev d, const float2* __restrict__ gV,
+                                                                         float2* __restrict__ Bt) {
+    extern __shared__ float2 sm[];
+    const int ld = fft_ld(d.NW);
+    const int row = blockIdx.x;
+    const int pc = row / d.out_h, y = row - pc * d.out_h;
+    const int col0 = (d.NW >> 1) - (d.out_w >> 1);
+    const int ow = d.out_w;
+    const float2* src = gV + (size_t)row * ow;
+    float2* res = fft_run(
+        [=](int, int e) {
+            const int x = e - col0;
+            return (x < 0 || x >= ow) ? make_float2(0.f, 0.f) : __ldg(&src[x]);
+        },
+        sm, sm + ld, ld, 0, d.row, false);
+    const int G = d.G, ngroups = d.NW / G;
+    for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) {
+        const int gi = kx / G, g = kx - gi * G;
+        Bt[(((size_t)pc * ngroups + gi) * d.out_h + y) * G + g] = res[fft_pad(kx)];
+    }
+}
+
+// K2b: per plane forward column FFT (first pass reads the tiled gradient rows),
+// multiply by conj(transfer) and accumulate in registers; then one inverse FFT
+// of the sum; keep the input rows -> Ab [C][in_h][NW]
+template <int G, int E>
+__global__ void __launch_bounds__(kColThreads, 1) blasm_cols_adj_kernel(BlasmDev d, const float2* __restrict__ Bt,
+                                                                        float2* __restrict__ Ab) {
+    extern __shared__ float2 sm[];
+    constexpr int TS = ilog2c(G);
+    const int ld = fft_ld(d.NH);
+    float2* b0 = sm;
+    float2* b1 = sm + G * ld;
+    const int ngroups = d.NW / G;
+    const int c = blockIdx.x / ngroups, gi = blockIdx.x - c * ngroups;
+    const int kx0 = gi * G;
+    const int row0 = (d.NH >> 1) - (d.out_h >> 1);
+    const int oh = d.out_h;
+    const int total = G * d.NH;
+    float2 acc[E];
+#pragma unroll
+    for (int i = 0; i < E; i++) acc[i] = make_float2(0.f, 0.f);
+    for (int p = 0; p < d.P; p++) {
+        const int pc = p * d.C + c;
+        const float2* src = Bt + ((size_t)pc * ngroups + gi) * oh * G;
+        float2* res = fft_run(
+            [=](int t, int e) {
+                const int y = e - row0;
+                return (y < 0 || y >= oh) ? make_float2(0.f, 0.f) : __ldg(&src[y * G + t]);
+            },
+            b0, b1, ld, TS, d.col, false);
+        const PCParam pp = d.pcp[pc];
+#pragma unroll
+        for (int i = 0; i < E; i++) {
+            const int e = threadIdx.x + i * blockDim.x;
+            if (e < total) {
+                const int t = e & (G - 1), ky = e >> TS;
+                acc[i] = cadd(acc[i], cmulc(res[t * ld + fft_pad(ky)], transfer(d, pp, c, ky, kx0 + t)));
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < E; i++) {
+        const int e = threadIdx.x + i * blockDim.x;
+        if (e < total) {
+            const int t = e & (G - 1), ky = e >> TS;
+            b0[t * ld + fft_pad(ky)] = acc[i];
+        }
+    }
+    __syncthreads();
+    const float2* s0 = b0;
+    float2* res = fft_run([=](int t, int e) { return s0[t * ld + fft_pad(e)]; }, b1, b0, ld, TS, d.col, true);
+    const int in_h = d.input_mode == 0 ? d.H : d.pH;
+    const int r0 = (d.NH >> 1) - (in_h >> 1);
+    float2* dst = Ab + (size_t)c * in_h * d.NW + kx0;
+    for (int e = threadIdx.x; e < in_h * G; e += blockDim.x) {
+        const int y = e >> TS, g = e & (G - 1);
+        dst[(size_t)y * d.NW + g] = res[g * ld + fft_pad(r0 + y)];
+    }
+}
+
+// K1b: inverse row FFT (first pass reads global), keep the input columns,
+// apply the amplitude-clamp adjoint against the splat field
+__global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_adj_kernel(BlasmDev d, const float2* __restrict__ Ab,
+                                                                         const float2* __restrict__ field,
+                                                                         float2* __restrict__ gin) {
+    extern __shared__ float2 sm[];
+    const int ld = fft_ld(d.NW);
+    const int row = blockIdx.x;  // c * in_h + y
+    const float2* src = Ab + (size_t)row * d.NW;
+    float2* res = fft_run([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, 0, d.row, true);
+    const int in_w = d.input_mode == 0 ? d.W : d.pW;
+    const int c0 = (d.NW >> 1) - (in_w >> 1);
+    float2* dst = gin + (size_t)row * in_w;
+    if (d.input_mode == 0) {
+        const float2* u = field + (size_t)row * d.W;  // the window is exactly 1 over the image
+        for (int x = threadIdx.x; x < d.W; x += blockDim.x)
+            dst[x] = clamp_amplitude_adjoint(u[x], res[fft_pad(c0 + x)]);
+    } else {
+        for (int x = threadIdx.x; x < in_w; x += blockDim.x) dst[x] = res[fft_pad(c0 + x)];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host: table blob, device config, launches
+// ---------------------------------------------------------------------------
+struct TableLayout {
+    size_t tw_row, tw_col, wy, wx, a_row, b_col, aperture, pcp, total;
+};
+
+static TableLayout table_layout(int C, int P, int pH, int pW) {
+    TableLayout L;
+    const int NH = 2 * pH, NW = 2 * pW;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        off = (off + 255) & ~(size_t)255;
+        size_t o = off;
+        off += bytes;
+        return o;
+    };
+    L.tw_row = take(sizeof(float2) * NW);
+    L.tw_col = take(sizeof(float2) * NH);
+    L.wy = take(sizeof(float) * pH);
+    L.wx = take(sizeof(float) * pW);
+    L.a_row = take(sizeof(float) * C * NH);
+    L.b_col = take(sizeof(float) * C * NW);
+    L.aperture = take(sizeof(int2) * NH);
+    L.pcp = take(sizeof(PCParam) * P * C);
+    L.total = off;
+    return L;
+}
+
+static int validate(const cvqpg_blasm_params* p) {
+    if (!p) return CVQPG_ERR_ARG;
+    if (p->channels != 1 && p->channels != 3) return CVQPG_ERR_CHANNELS;
+    if (p->planes < 1 || p->planes > kMaxPlanes) return CVQPG_ERR_UNSUPPORTED;
+    const int H = p->height, W = p->width, pH = p->pad_height, pW = p->pad_width;
+    if (H <= 0 || W <= 0 || pH < H || pW < W) return CVQPG_ERR_ARG;
+    if ((H | W | pH | pW) & 1) return CVQPG_ERR_UNSUPPORTED;
+    const int oh = p->out_height > 0 ? p->out_height : H, ow = p->out_width > 0 ? p->out_width : W;
+    if (oh > pH || ow > pW || ((oh | ow) & 1)) return CVQPG_ERR_UNSUPPORTED;
+    if (p->input_mode != 0 && p->input_mode != 1) return CVQPG_ERR_ARG;
+    if (!(p->pixel_pitch > 0)) return CVQPG_ERR_ARG;
+    FftPlan a, b;
+    if (!make_fft_plan(2 * pH, &a) || !make_fft_plan(2 * pW, &b)) return CVQPG_ERR_UNSUPPORTED;
+    return CVQPG_OK;
+}
+
+// Tukey taper of the reference soft_window_pad (_taper_1d, model_2d_gaussian_rgb.py:224-235)
+static void taper_1d(int total, int inner_start, int inner_size, float* w) {
+    for (int t = 0; t < total; t++) w[t] = 0.0f;
+    for (int t = inner_start; t < inner_start + inner_size; t++) w[t] = 1.0f;
+    for (int t = 0; t < inner_start; t++) w[t] = (float)(0.5 * (1.0 - cos(M_PI * (t + 1.0) / inner_start)));
+    const int right = inner_start + inner_size, n_right = total - right;
+    for (int t = 0; t < n_right; t++) w[right + t] = (float)(0.5 * (1.0 + cos(M_PI * (t + 1.0) / n_right)));
+}
+
+// symmetric frequency sample j of an n-point axis (odak BLASM grid convention, see oracle/odak_restated.py)
+static double freq(int j, int n, double dx) {
+    const double s = dx * n;
+    const double a = -1.0 / (2.0 * dx) + 0.5 / (2.0 * s);
+    const double b = 1.0 / (2.0 * dx) - 0.5 / (2.0 * s);
+    return a + (b - a) * (double)j / (double)(n - 1);
+}
+
+static void band_interval(int n, double dx, double lim, int* lo, int* hi) {
+    int a = n, b = 0;
+    for (int j = 0; j < n; j++)
+        if (fabs(freq(j, n, dx)) < lim) {
+            a = std::min(a, j);
+            b = std::max(b, j + 1);
+        }
+    if (a >= b) a = b = 0;
+    *lo = a;
+    *hi = b;
+}
+
+int blasm_make_dev(const cvqpg_blasm_params* p, const void* tables, size_t table_bytes, BlasmDev* d) {
+    int st = validate(p);
+    if (st != CVQPG_OK) return st;
+    const int C = p->channels, P = p->planes;
+    TableLayout L = table_layout(C, P, p->pad_height, p->pad_width);
+    if (!tables || table_bytes < L.total) return CVQPG_ERR_WORKSPACE;
+    std::memset(d, 0, sizeof(*d));
+    d->C = C;
+    d->P = P;
+    d->H = p->height;
+    d->W = p->width;
+    d->pH = p->pad_height;
+    d->pW = p->pad_width;
+    d->NH = 2 * d->pH;
+    d->NW = 2 * d->pW;
+    d->pad_h = (d->pH - d->H) / 2;
+    d->pad_w = (d->pW - d->W) / 2;
+    d->out_h = p->out_height > 0 ? p->out_height : d->H;
+    d->out_w = p->out_width > 0 ? p->out_width : d->W;
+    d->input_mode = p->input_mode;
+    // columns per column-pass CTA: the widest of 2, 1 whose three ping-pong
+    // buffers fit in shared memory
+    d->G = (size_t)3 * 2 * fft_ld(d->NH) * sizeof(float2) <= 227 * 1024 ? 2 : 1;
+    if ((size_t)3 * d->G * fft_ld(d->NH) * sizeof(float2) > 227 * 1024) return CVQPG_ERR_UNSUPPORTED;
+    if (d->NW % d->G) return CVQPG_ERR_UNSUPPORTED;
+    d->scale = (float)(1.0 / ((double)d->NH * (double)d->NW));
+    make_fft_plan(d->NW, &d->row);
+    make_fft_plan(d->NH, &d->col);
+    const char* base = (const char*)tables;
+    d->row.tw = (const float2*)(base + L.tw_row);
+    d->col.tw = (const float2*)(base + L.tw_col);
+    d->wy = (const float*)(base + L.wy);
+    d->wx = (const float*)(base + L.wx);
+    d->a_row = (const float*)(base + L.a_row);
+    d->b_col = (const float*)(base + L.b_col);
+    d->aperture = (const int2*)(base + L.aperture);
+    d->pcp = (const PCParam*)(base + L.pcp);
+    return CVQPG_OK;
+}
+
+size_t blasm_workspace_bytes(const BlasmDev& d) {
+    const size_t a = (size_t)d.C * d.NW * d.pH;
+    const size_t b = (size_t)d.P * d.C * d.out_h * d.NW;
+    return ((a * sizeof(float2) + 255) & ~(size_t)255) + b * sizeof(float2) + 256;
+}
+
+static void carve(const BlasmDev& d, void* ws, float2** A, float2** B) {
+    const size_t a = (size_t)d.C * d.NW * d.pH;
+    *A = (float2*)ws;
+    *B = (float2*)((char*)ws + ((a * sizeof(float2) + 255) & ~(size_t)255));
+}
+
+static size_t row_smem(const BlasmDev& d) { return (size_t)2 * fft_ld(d.NW) * sizeof(float2); }
+static size_t col_fwd_smem(const BlasmDev& d) { return (size_t)3 * d.G * fft_ld(d.NH) * sizeof(float2); }
+static size_t col_adj_smem(const BlasmDev& d) { return (size_t)2 * d.G * fft_ld(d.NH) * sizeof(float2); }
+constexpr size_t kSmemMax = 227 * 1024;
+
+#define CVQPG_SMEM_ATTR(kern, bytes) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(bytes))
+
+template <int G>
+static void launch_cols_fwd(const BlasmDev& d, const float2* A, float2* B, cudaStream_t s) {
+    const size_t sm = col_fwd_smem(d);
+    CVQPG_SMEM_ATTR(blasm_cols_fwd_kernel<G>, sm);
+    blasm_cols_fwd_kernel<G><<<d.C * (d.NW / G), kColThreads, sm, s>>>(d, A, B);
+}
+
+template <int G, int E>
+static void launch_cols_adj(const BlasmDev& d, const float2* Bt, float2* Ab, cudaStream_t s) {
+    const size_t sm = col_adj_smem(d);
+    CVQPG_SMEM_ATTR((blasm_cols_adj_kernel<G, E>), sm);
+    blasm_cols_adj_kernel<G, E><<<d.C * (d.NW / G), kColThreads, sm, s>>>(d, Bt, Ab);
+}
+
+template <int G>
+static void dispatch_cols_adj(const BlasmDev& d, const float2* Bt, float2* Ab, cudaStream_t s) {
+    const int e = (G * d.NH + kColThreads - 1) / kColThreads;
+    if (e <= 8) launch_cols_adj<G, 8>(d, Bt, Ab, s);
+    else if (e <= 16) launch_cols_adj<G, 16>(d, Bt, Ab, s);
+    else launch_cols_adj<G, 32>(d, Bt, Ab, s);
+}
+
+void blasm_forward(const BlasmDev& d, const float2* in, float2* out, void* workspace, cudaStream_t s) {
+    float2 *A, *B;
+    carve(d, workspace, &A, &B);
+    const size_t rs = row_smem(d);
+    CVQPG_SMEM_ATTR(blasm_rows_fwd_kernel, rs);
+    blasm_rows_fwd_kernel<<<d.C * d.pH, kRowThreads, rs, s>>>(d, in, A);
+    if (d.G == 4) launch_cols_fwd<4>(d, A, B, s);
+    else if (d.G == 2) launch_cols_fwd<2>(d, A, B, s);
+    else launch_cols_fwd<1>(d, A, B, s);
+    CVQPG_SMEM_ATTR(blasm_rows_inv_kernel, rs);
+    blasm_rows_inv_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, B, out);
+}
+
+void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* grad_out, float2* grad_in,
+                    void* workspace, cudaStream_t s) {
+    float2 *A, *B;
+    carve(d, workspace, &A, &B);
+    const size_t rs = row_smem(d);
+    CVQPG_SMEM_ATTR(blasm_rows_fwd_adj_kernel, rs);
+    blasm_rows_fwd_adj_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, grad_out, B);
+    if (d.G == 4) dispatch_cols_adj<4>(d, B, A, s);
+    else if (d.G == 2) dispatch_cols_adj<2>(d, B, A, s);
+    else dispatch_cols_adj<1>(d, B, A, s);
+    const int in_h = d.input_mode == 0 ? d.H : d.pH;
+    CVQPG_SMEM_ATTR(blasm_rows_inv_adj_kernel, rs);
+    blasm_rows_inv_adj_kernel<<<d.C * in_h, kRowThreads, rs, s>>>(d, A, in_field, grad_in);
+}
+
+static bool fits(const BlasmDev& d) {
+    return row_smem(d) <= kSmemMax && col_fwd_smem(d) <= kSmemMax &&
+           (d.G * d.NH + kColThreads - 1) / kColThreads <= 32;
+}
+
+}  // namespace cvqpg
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace cvqpg;
+
+extern "C" int cvqpg_blasm_tables_size(const cvqpg_blasm_params* p, size_t* bytes) {
+    if (!bytes) return CVQPG_ERR_ARG;
+    int st = validate(p);
+    if (st != CVQPG_OK) return st;
+    *bytes = table_layout(p->channels, p->planes, p->pad_height, p->pad_width).total;
+    return CVQPG_OK;
+}
+
+extern "C" int cvqpg_blasm_setup(const cvqpg_blasm_params* p, void* tables, size_t table_bytes) {
+    int st = validate(p);
+    if (st != CVQPG_OK) return st;
+    const int C = p->channels, P = p->planes, pH = p->pad_height, pW = p->pad_width;
+    const int H = p->height, W = p->width, NH = 2 * pH, NW = 2 * pW;
+    TableLayout L = table_layout(C, P, pH, pW);
+    if (!tables || table_bytes < L.total) return CVQPG_ERR_WORKSPACE;
+    std::vector<char> host(L.total, 0);
+    char* b = host.data();
+    auto twiddles = [](int n, float2* t) {
+        for (int m = 0; m < n; m++) {
+            const double a = -2.0 * M_PI * (double)m / (double)n;
+            t[m] = make_float2((float)cos(a), (float)sin(a));
+        }
+    };
+    twiddles(NW, (float2*)(b + L.tw_row));
+    twiddles(NH, (float2*)(b + L.tw_col));
+    taper_1d(pH, (pH - H) / 2, H, (float*)(b + L.wy));
+    taper_1d(pW, (pW - W) / 2, W, (float*)(b + L.wx));
+    const double dx = p->pixel_pitch;
+    float* ar = (float*)(b + L.a_row);
+    float* bc = (float*)(b + L.b_col);
+    for (int c = 0; c < C; c++) {
+        const double lam = p->wavelengths[c];
+        for (int j = 0; j < NH; j++) {
+            const double f = freq(j, NH, dx);
+            ar[c * NH + j] = (float)(lam * lam * f * f);
+        }
+        for (int i = 0; i < NW; i++) {
+            const double f = freq(i, NW, dx);
+            bc[c * NW + i] = (float)(lam * lam * f * f);
+        }
+    }
+    // circular Fourier aperture (utils/propagator.py:10-38, 179-200): per centred row j the
+    // allowed centred columns i satisfy sqrt(X_j^2 + Y_i^2) < r, X = linspace(-NH/2, NH/2, NH)
+    int2* ap = (int2*)(b + L.aperture);
+    const double r = p->aperture_radius;
+    for (int j = 0; j < NH; j++) {
+        if (!(r > 0)) {
+            ap[j] = make_int2(0, NW);
+            continue;
+        }
+        const double X = -NH / 2.0 + (double)NH * j / (NH - 1.0);
+        int lo = NW, hi = 0;
+        for (int i = 0; i < NW; i++) {
+            const double Y = -NW / 2.0 + (double)NW * i / (NW - 1.0);
+            if (sqrt(X * X + Y * Y) < r) {
+                lo = std::min(lo, i);
+                hi = std::max(hi, i + 1);
+            }
+        }
+        ap[j] = lo < hi ? make_int2(lo, hi) : make_int2(0, 0);
+    }
+    PCParam* pcp = (PCParam*)(b + L.pcp);
+    for (int pl = 0; pl < P; pl++)
+        for (int c = 0; c < C; c++) {
+            const double lam = p->wavelengths[c], z = p->distances[pl];
+            PCParam q;
+            std::memset(&q, 0, sizeof(q));
+            const double K = 2.0 * M_PI * z / lam;
+            q.K = (float)K;
+            double t0 = fmod(K, 2.0 * M_PI);
+            if (t0 < 0) t0 += 2.0 * M_PI;
+            q.theta0 = (float)t0;
+            const double lim_r = 1.0 / sqrt(pow(2.0 * z * (1.0 / (dx * NH)), 2) + 1.0) / lam;
+            const double lim_c = 1.0 / sqrt(pow(2.0 * z * (1.0 / (dx * NW)), 2) + 1.0) / lam;
+            band_interval(NH, dx, lim_r, &q.j0, &q.j1);
+            band_interval(NW, dx, lim_c, &q.i0, &q.i1);
+            pcp[pl * C + c] = q;
+        }
+    if (cudaMemcpy(tables, host.data(), L.total, cudaMemcpyHostToDevice) != cudaSuccess) return CVQPG_ERR_CUDA;
+    return CVQPG_OK;
+}
+
+extern "C" int cvqpg_blasm_workspace_size(const cvqpg_blasm_params* p, size_t* bytes) {
+    if (!bytes) return CVQPG_ERR_ARG;
+    int st = validate(p);
+    if (st != CVQPG_OK) return st;
+    BlasmDev d;
+    static const char dummy[1] = {0};
+    st = blasm_make_dev(p, dummy, (size_t)-1, &d);
+    if (st != CVQPG_OK) return st;
+    *bytes = blasm_workspace_bytes(d);
+    return CVQPG_OK;
+}
+
+extern "C" int cvqpg_blasm_forward(const cvqpg_blasm_params* p, const void* tables, size_t table_bytes,
+                                   const float* input, float* out_field, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+    BlasmDev d;
+    int st = blasm_make_dev(p, tables, table_bytes, &d);
+    if (st != CVQPG_OK) return st;
+    if (!fits(d)) return CVQPG_ERR_UNSUPPORTED;
+    if (!input || !out_field || !workspace) return CVQPG_ERR_ARG;
+    if (workspace_bytes < blasm_workspace_bytes(d)) return CVQPG_ERR_WORKSPACE;
+    blasm_forward(d, (const float2*)input, (float2*)out_field, workspace, (cudaStream_t)stream);
+    return launch_status();
+}
+
+extern "C" int cvqpg_blasm_backward(const cvqpg_blasm_params* p, const void* tables, size_t table_bytes,
+                                    const float* input, const float* grad_out, float* grad_input, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+    BlasmDev d;
+    int st = blasm_make_dev(p, tables, table_bytes, &d);
+    if (st != CVQPG_OK) return st;
+    if (!fits(d)) return CVQPG_ERR_UNSUPPORTED;
+    if (!grad_out || !grad_input || !workspace || (d.input_mode == 0 && !input)) return CVQPG_ERR_ARG;
+    if (workspace_bytes < blasm_workspace_bytes(d)) return CVQPG_ERR_WORKSPACE;
+    blasm_backward(d, (const float2*)input, (const float2*)grad_out, (float2*)grad_input, workspace,
+                   (cudaStream_t)stream);
+    return launch_status();
+}

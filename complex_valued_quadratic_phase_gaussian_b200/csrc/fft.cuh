@@ -1,0 +1,221 @@
+// Shared-memory mixed-radix FFT engine (Stockham autosort, radices 2..17).
+//
+// A CTA transforms `ntrans` sequences of length n that live in shared memory
+// (sequence t at buf + t*ld, element a at index fft_pad(a)). Passes are out of
+// place between two buffers, so a thread only ever holds one butterfly in
+// registers. The padding (one slot every 32 elements) breaks the power-of-two
+// strides of the early passes into distinct banks.
+//
+// Pass s with radix R and Ns = product of the previous radices computes, for
+// every butterfly j in [0, n/R):   k = j mod Ns,
+//   v_r = x[j + r*n/R] * W_n^(r*k*n/(Ns*R)),  V = DFT_R(v),
+//   y[(j/Ns)*Ns*R + k + r*Ns] = V_r
+// (the textbook Stockham formulation, e.g. C. Van Loan, "Computational
+// Frameworks for the Fast Fourier Transform", SIAM 1992, sec. 1.7). Forward
+// transforms use W_n = exp(-2 pi i / n) (the numpy/torch fft sign), inverse
+// ones exp(+2 pi i / n) without the 1/n factor.
+#pragma once
+
+#include "common.cuh"
+#include "dft_tables.cuh"
+
+namespace cvqpg {
+
+constexpr int kMaxPasses = 8;
+
+struct FftPlan {
+    int n;
+    int npass;
+    unsigned long long code;  // radix of pass p in bits [5p, 5p+5)
+    const float2* tw;         // device table W_n^m = exp(-2 pi i m / n), m in [0, n)
+};
+
+__host__ __device__ __forceinline__ int fft_pad(int i) { return i + (i >> 5); }
+__host__ __device__ __forceinline__ int fft_ld(int n) { return fft_pad(n - 1) + 2; }
+
+// ---------------------------------------------------------------------------
+// small DFTs on registers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 mul_i(float2 a, bool neg) {  // neg ? -i*a : +i*a
+    return neg ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+}
+
+__device__ __forceinline__ void dft4(float2& x0, float2& x1, float2& x2, float2& x3, bool inv) {
+    const float2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = csub(x1, x3);
+    const float2 r = mul_i(t3, !inv);  // forward: -i*t3
+    x0 = cadd(t0, t2);
+    x2 = csub(t0, t2);
+    x1 = cadd(t1, r);
+    x3 = csub(t1, r);
+}
+
+template <int R>
+__device__ __forceinline__ void dft(float2 (&v)[R], bool inv) {
+    if constexpr (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        dft4(v[0], v[1], v[2], v[3], inv);
+    } else if constexpr (R == 8) {
+        float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+        float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+        dft4(e0, e1, e2, e3, inv);
+        dft4(o0, o1, o2, o3, inv);
+        float2 e[4] = {e0, e1, e2, e3}, o[4] = {o0, o1, o2, o3};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float2 w = make_float2(DftTab<8>::c(k), inv ? DftTab<8>::s(k) : -DftTab<8>::s(k));
+            const float2 t = k == 0 ? o[0] : cmul(o[k], w);
+            v[k] = cadd(e[k], t);
+            v[k + 4] = csub(e[k], t);
+        }
+    } else if constexpr (R == 16) {
+        float2 y[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; n2++) {
+            y[n2][0] = v[n2];
+            y[n2][1] = v[4 + n2];
+            y[n2][2] = v[8 + n2];
+            y[n2][3] = v[12 + n2];
+            dft4(y[n2][0], y[n2][1], y[n2][2], y[n2][3], inv);
+#pragma unroll
+            for (int k1 = 1; k1 < 4; k1++) {
+                if (n2 == 0) continue;
+                const int q = (n2 * k1) & 15;
+                const float2 w = make_float2(DftTab<16>::c(q), inv ? DftTab<16>::s(q) : -DftTab<16>::s(q));
+                y[n2][k1] = cmul(y[n2][k1], w);
+            }
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < 4; k1++) {
+            float2 a = y[0][k1], b = y[1][k1], c = y[2][k1], d = y[3][k1];
+            dft4(a, b, c, d, inv);
+            v[k1] = a;
+            v[k1 + 4] = b;
+            v[k1 + 8] = c;
+            v[k1 + 12] = d;
+        }
+    } else {
+        // odd R: X_k = x0 + sum_m (x_m + x_{R-m}) cos(2 pi m k/R) -/+ i (x_m - x_{R-m}) sin(2 pi m k/R)
+        static_assert(R % 2 == 1, "odd radix expected");
+        constexpr int h = (R - 1) / 2;
+        float2 a[h], b[h];
+        float2 sum = v[0];
+#pragma unroll
+        for (int m = 1; m <= h; m++) {
+            a[m - 1] = cadd(v[m], v[R - m]);
+            b[m - 1] = csub(v[m], v[R - m]);
+            sum = cadd(sum, a[m - 1]);
+        }
+        float2 out[R];
+        out[0] = sum;
+#pragma unroll
+        for (int k = 1; k <= h; k++) {
+            float2 A = v[0], B = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int m = 1; m <= h; m++) {
+                const int q = (m * k) % R;
+                A.x = fmaf(a[m - 1].x, DftTab<R>::c(q), A.x);
+                A.y = fmaf(a[m - 1].y, DftTab<R>::c(q), A.y);
+                B.x = fmaf(b[m - 1].x, DftTab<R>::s(q), B.x);
+                B.y = fmaf(b[m - 1].y, DftTab<R>::s(q), B.y);
+            }
+            if (!inv) {
+                out[k] = make_float2(A.x + B.y, A.y - B.x);
+                out[R - k] = make_float2(A.x - B.y, A.y + B.x);
+            } else {
+                out[k] = make_float2(A.x - B.y, A.y + B.x);
+                out[R - k] = make_float2(A.x + B.y, A.y - B.x);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = out[r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// one out-of-place Stockham pass over `ntrans` sequences. `src(t, a)` returns
+// element a of sequence t (a plain shared-memory read for every pass but the
+// first, where it can fuse a pointwise multiply into the load). Each thread
+// holds a single butterfly at a time, so the register footprint is one radix.
+// ---------------------------------------------------------------------------
+template <int R, typename Src>
+__device__ __forceinline__ void fft_pass(Src src, float2* __restrict__ out, int ld, int tshift, int n, int Ns,
+                                         const float2* __restrict__ tw, bool inv) {
+    const int nb = n / R;
+    const int total = nb << tshift;
+    const int stride = n / (Ns * R);
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int t = idx & ((1 << tshift) - 1), j = idx >> tshift;  // sequences interleaved across lanes
+        const int k = j % Ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = src(t, j + r * nb);
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                float2 w = __ldg(&tw[r * k * stride]);
+                if (inv) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        dft<R>(v, inv);
+        const int o = (j / Ns) * Ns * R + k;
+        float2* dst = out + t * ld;
+#pragma unroll
+        for (int r = 0; r < R; r++) dst[fft_pad(o + r * Ns)] = v[r];
+    }
+    __syncthreads();
+}
+
+template <typename Src>
+__device__ __forceinline__ void fft_pass_dispatch(int R, Src src, float2* out, int ld, int tshift, int n, int Ns,
+                                                  const float2* tw, bool inv) {
+    switch (R) {
+        case 16: fft_pass<16>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 8: fft_pass<8>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 4: fft_pass<4>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 2: fft_pass<2>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 3: fft_pass<3>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 5: fft_pass<5>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 7: fft_pass<7>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 11: fft_pass<11>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 13: fft_pass<13>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 17: fft_pass<17>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        default: break;
+    }
+}
+
+// Full transform of 2^tshift sequences with ping-pong buffers a, b. The first
+// pass reads through `first` and writes a; later passes alternate. Returns the
+// buffer holding the result (a or b). The caller must synchronise before
+// `first` reads anything written earlier; the function ends with a barrier.
+template <typename First>
+__device__ __forceinline__ float2* fft_run(First first, float2* a, float2* b, int ld, int tshift, FftPlan plan,
+                                           bool inv) {
+    const int n = plan.n;
+    int Ns = 1;
+    int R = (int)(plan.code & 31ull);
+    fft_pass_dispatch(R, first, a, ld, tshift, n, Ns, plan.tw, inv);
+    Ns *= R;
+    float2* cur = a;
+    float2* nxt = b;
+    for (int p = 1; p < plan.npass; p++) {
+        R = (int)((plan.code >> (5 * p)) & 31ull);
+        const float2* in = cur;
+        fft_pass_dispatch(R, [in, ld](int t, int e) { return in[t * ld + fft_pad(e)]; }, nxt, ld, tshift, n, Ns,
+                          plan.tw, inv);
+        Ns *= R;
+        float2* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+    return cur;
+}
+
+// Host: factor n into supported radices (16/8/4/2 first, then 3..17).
+// Returns false when n has a prime factor above 17.
+bool make_fft_plan(int n, FftPlan* plan);
+
+}  // namespace cvqpg

@@ -132,6 +132,60 @@ CVQPG_API int cvqpg_render_backward_cull(const float* grad_field, const float* m
                                          float* d_opacities, float* d_curvature, float* d_area,
                                          void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- band-limited angular-spectrum propagation (BLASM) --------------------
+ *
+ * Replaces, for one hologram, the reference chain
+ *   soft_window_pad                (model_2d_gaussian_rgb.py:186-241)
+ *   angle % 2pi, clamp(|U|, 0, 1)  (train_2d_gaussian_rgb.py:89-95)
+ *   propagator._reconstruct_impl   (utils/propagator.py:248-290; custom() :41-64;
+ *                                   transfer functions :202-222, aperture :179-200)
+ *   crop_center to the image       (train_2d_gaussian_rgb.py:193)
+ * with every plane and wavelength in one sequence of three kernels:
+ *   rows   : pad/window/clamp + forward FFT of the pH nonzero rows (length 2pW)
+ *   columns: forward FFT (length 2pH) once, then per plane the transfer-function
+ *            multiply (computed on the fly) and the inverse FFT, keeping only
+ *            the output rows
+ *   rows   : inverse FFT of the kept rows, keeping only the output columns.
+ * Output: the complex field V [P, C, out_h, out_w] (the reference intensity is
+ * |V|^2). The adjoint applies the same kernels with the conjugate transfer
+ * function, summed over planes.
+ *
+ * input_mode 0: input = splat field [C, H, W] (complex64); the kernel applies
+ *               the replicate guard band, Tukey window and amplitude clamp.
+ *               The adjoint returns dL/d(splat field) [C, H, W] (the guard band
+ *               carries no gradient, as in the reference).
+ * input_mode 1: input = already-padded complex field [C, pH, pW]; the adjoint
+ *               returns dL/d(input) [C, pH, pW].
+ * Requirements: even H, W, pH, pW with pH >= H, pW >= W; 2pH and 2pW products
+ * of primes <= 17; planes <= 8; channels 1 or 3.
+ */
+typedef struct cvqpg_blasm_params {
+    int channels;
+    int planes;
+    int height, width;          /* image H, W                                  */
+    int pad_height, pad_width;  /* pH, pW (the reference pad_size)             */
+    int out_height, out_width;  /* output crop; 0 = (H, W)                     */
+    int input_mode;             /* 0 or 1, see above                           */
+    int reserved;
+    double pixel_pitch;         /* metres                                      */
+    double wavelengths[3];      /* metres, one per channel                     */
+    double distances[8];        /* metres, one per plane                       */
+    double aperture_radius;     /* Fourier aperture radius on the 2x grid (px);
+                                   <= 0 disables it                            */
+} cvqpg_blasm_params;
+
+/* Device table blob (twiddles, windows, frequency tables, band limits):
+ * size query, then a synchronous host-side fill of a caller buffer. */
+CVQPG_API int cvqpg_blasm_tables_size(const cvqpg_blasm_params* prm, size_t* bytes);
+CVQPG_API int cvqpg_blasm_setup(const cvqpg_blasm_params* prm, void* tables, size_t table_bytes);
+CVQPG_API int cvqpg_blasm_workspace_size(const cvqpg_blasm_params* prm, size_t* bytes);
+CVQPG_API int cvqpg_blasm_forward(const cvqpg_blasm_params* prm, const void* tables, size_t table_bytes,
+                                  const float* input, float* out_field, void* workspace,
+                                  size_t workspace_bytes, void* stream);
+CVQPG_API int cvqpg_blasm_backward(const cvqpg_blasm_params* prm, const void* tables, size_t table_bytes,
+                                   const float* input, const float* grad_out, float* grad_input,
+                                   void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

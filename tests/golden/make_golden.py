@@ -233,6 +233,36 @@ def golden_torch_renderer(C, name, seed, n=400, W=160, H=112, pad=(176, 224)):
                         grad_field=f2.grad.numpy(), **grads, **act)
 
 
+def golden_propagate(C, name, seed, H, W, pH, pW, P, d_val, vd, aperture_size):
+    """soft_window_pad -> phase/amplitude -> propagator.reconstruct -> crop (train_2d_gaussian_rgb.py:89-95, 193)."""
+    model = load_by_path(f"ref_model_{C}", ref("model_2d_gaussian_rgb.py" if C == 3 else
+                                              "model_2d_gaussian_grayscale.py"))
+    prop_mod = load_by_path("ref_propagator", ref("utils/propagator.py"))
+    import odak
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.0, 1.35, (C, H, W))
+    field = (amp * np.exp(1j * rng.uniform(0, 2 * np.pi, (C, H, W)))).astype(np.complex64)
+    field[0, 3, 5] = 0.0  # exact zero: the clamp/angle adjoint returns 0 there
+    wl = WAVELENGTHS if C == 3 else WAVELENGTHS[:1]
+    distances = torch.linspace(-vd / 2.0, vd / 2.0, P) + d_val if P > 1 else torch.tensor([d_val])
+    prop = prop_mod.propagator(resolution=[pH, pW], wavelengths=wl, pixel_pitch=PITCH, number_of_frames=C,
+                               distances=distances, propagation_type="Bandlimited Angular Spectrum",
+                               laser_channel_power=torch.eye(C), aperture_size=aperture_size, device="cpu")
+    f = torch.from_numpy(field).requires_grad_(True)
+    U = model.soft_window_pad(f, [pH, pW])
+    phase = odak.learn.wave.calculate_phase(U) % (2 * odak.pi)
+    amplitude = torch.clamp(odak.learn.wave.calculate_amplitude(U), min=0.0, max=1.0)
+    rec = prop.reconstruct(phase, amplitude=amplitude, no_grad=False)
+    I_full = torch.sum(rec, dim=0)
+    I_crop = odak.learn.tools.crop_center(I_full, size=(H, W))
+    wts = torch.from_numpy(rng.normal(0, 1, (P, C, H, W)).astype(np.float32))
+    (I_crop * wts).sum().backward()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), field=field, H=H, W=W, pH=pH, pW=pW,
+                        distances=distances.double().numpy(), wavelengths=np.array(wl), pitch=PITCH,
+                        aperture=float(aperture_size), I_full=I_full.detach().numpy(),
+                        I_crop=I_crop.detach().numpy(), wts=wts.numpy(), grad_field=f.grad.numpy())
+
+
 GOLDENS = {
     "splat_rgb": lambda: golden_splat(3, "splat_rgb", 11),
     "splat_gray": lambda: golden_splat(1, "splat_gray", 12),
@@ -240,6 +270,11 @@ GOLDENS = {
     "preprocess_gray": lambda: golden_preprocess(1, "preprocess_gray", 22),
     "torch_renderer_rgb": lambda: golden_torch_renderer(3, "torch_renderer_rgb", 31),
     "torch_renderer_gray": lambda: golden_torch_renderer(1, "torch_renderer_gray", 32),
+    # 2pH = 176 = 16*11, 2pW = 208 = 16*13, 3 planes, aperture wide open (train default 10*max(img))
+    "propagate_rgb": lambda: golden_propagate(3, "propagate_rgb", 41, 40, 56, 88, 104, 3, 1e-3, 1e-3, 560),
+    # 2pH = 2pW = 120 = 8*3*5: band limit active (z = 5 cm) and a small Fourier aperture
+    "propagate_gray_bandlimit": lambda: golden_propagate(1, "propagate_gray_bandlimit", 42, 32, 32, 60, 60, 2,
+                                                         5e-2, 2e-2, 40),
 }
 
 

@@ -1,0 +1,110 @@
+"""GPU parity of the fused pad/clamp/BLASM kernels and their adjoint.
+
+Gates: per-plane intensity within 1e-4 relative L2 of the reference propagator
+chain (golden fixtures); complex field within 2e-5 of the float64 oracle;
+gradients within 1e-4 of the reference autograd.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from oracle import blasm as ob
+
+pytestmark = pytest.mark.gpu
+CASES = ["propagate_rgb", "propagate_gray_bandlimit"]
+
+
+def _plan(g, **kw):
+    from complex_valued_quadratic_phase_gaussian_b200.propagator import BlasmPlan
+    C, H, W = g["field"].shape
+    return BlasmPlan(C, H, W, (int(g["pH"]), int(g["pW"])), list(g["wavelengths"]), list(g["distances"]),
+                     float(g["pitch"]), aperture_radius=float(g["aperture"]), **kw)
+
+
+def _oargs(g):
+    return int(g["pH"]), int(g["pW"]), list(g["wavelengths"]), list(g["distances"]), float(g["pitch"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_forward_and_adjoint_vs_reference(golden, name):
+    g = golden(name)
+    plan = _plan(g)
+    field = torch.from_numpy(g["field"]).cuda()
+    V = plan.forward(field)
+    Vn = V.cpu().numpy()
+    assert rel_l2(np.abs(Vn) ** 2, g["I_crop"]) < 1e-4
+    pH, pW, wl, dist, dx = _oargs(g)
+    Vo = ob.chain_forward(g["field"].astype(np.complex128), pH, pW, wl, dist, dx, aperture_radius=float(g["aperture"]))
+    assert rel_l2(Vn, Vo) < 2e-5
+    gV = (2.0 * V * torch.from_numpy(g["wts"]).cuda()).contiguous()
+    gf = plan.backward(field, gV).cpu().numpy()
+    assert rel_l2(gf, g["grad_field"]) < 1e-4
+    go = ob.chain_backward(g["field"].astype(np.complex128), 2.0 * Vo * g["wts"], pH, pW, wl, dist, dx,
+                           aperture_radius=float(g["aperture"]))
+    assert rel_l2(gf, go) < 2e-5
+    assert gf[0, 3, 5] == 0
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_reference_propagator_class_full_output(golden, name):
+    from complex_valued_quadratic_phase_gaussian_b200.propagator import propagator
+    g = golden(name)
+    pH, pW, wl, dist, dx = _oargs(g)
+    C = g["field"].shape[0]
+    U = ob.soft_window_pad(g["field"].astype(np.complex128), pH, pW)
+    phase = torch.from_numpy(np.mod(np.angle(U), 2 * np.pi).astype(np.float32)).cuda()
+    amp = torch.from_numpy(np.clip(np.abs(U), 0, 1).astype(np.float32)).cuda()
+    prop = propagator(resolution=[pH, pW], wavelengths=wl, pixel_pitch=dx, number_of_frames=C,
+                      distances=torch.tensor(dist, dtype=torch.float64), laser_channel_power=torch.eye(C),
+                      aperture_size=float(g["aperture"]), device=torch.device("cuda"))
+    I = prop.reconstruct(phase, amplitude=amp).sum(0).cpu().numpy()
+    assert rel_l2(I, g["I_full"]) < 1e-4
+
+
+def _random_field(rng, C, H, W):
+    a = rng.uniform(0, 1.3, (C, H, W))
+    return (a * np.exp(1j * rng.uniform(0, 2 * np.pi, (C, H, W)))).astype(np.complex64)
+
+
+def test_grayscale_256_three_planes_vs_oracle_and_adjoint():
+    """The 256x256 grayscale geometry (pad 576, FFT 1152 = 2^7 * 9, planes 1.0/1.5/2.0 mm)."""
+    from complex_valued_quadratic_phase_gaussian_b200.propagator import BlasmPlan, reference_distances
+    rng = np.random.default_rng(1)
+    H = W = 256
+    dist = reference_distances(3, 1e-3, 1.5e-3)
+    plan = BlasmPlan(1, H, W, (576, 576), [515e-9], dist, 8e-6, aperture_radius=2560)
+    f = _random_field(rng, 1, H, W)
+    V = plan.forward(torch.from_numpy(f).cuda())
+    Vo = ob.chain_forward(f.astype(np.complex128), 576, 576, [515e-9], dist, 8e-6, aperture_radius=2560)
+    assert rel_l2(V.cpu().numpy(), Vo) < 2e-5
+    y = (rng.normal(size=V.shape) + 1j * rng.normal(size=V.shape)).astype(np.complex64)
+    # adjoint identity of the linear part (input mode 1 = no clamp)
+    plan1 = BlasmPlan(1, H, W, (576, 576), [515e-9], dist, 8e-6, aperture_radius=2560, input_mode=1)
+    x = _random_field(rng, 1, 576, 576)
+    Lx = plan1.forward(torch.from_numpy(x).cuda()).cpu().numpy().astype(np.complex128)
+    Lty = plan1.backward(None, torch.from_numpy(y).cuda()).cpu().numpy().astype(np.complex128)
+    lhs, rhs = np.vdot(y.astype(np.complex128), Lx), np.vdot(Lty, x.astype(np.complex128))
+    assert abs(lhs - rhs) < 1e-4 * abs(lhs)
+
+
+def test_rgb_1080p_three_planes_vs_oracle():
+    """1920x1080 RGB headline geometry: pad 1408x2240, FFT grid 2816 x 4480, 3 planes."""
+    from complex_valued_quadratic_phase_gaussian_b200.propagator import (BlasmPlan, reference_distances,
+                                                                         reference_pad_size)
+    rng = np.random.default_rng(2)
+    H, W = 1080, 1920
+    pad = reference_pad_size((W, H))
+    assert pad == [1408, 2240]
+    wl = [639e-9, 515e-9, 473e-9]
+    dist = reference_distances(3, 1e-3, 1e-3)
+    plan = BlasmPlan(3, H, W, pad, wl, dist, 3.74e-6, aperture_radius=19200)
+    f = _random_field(rng, 3, H, W)
+    V = plan.forward(torch.from_numpy(f).cuda()).cpu().numpy()
+    Vo = ob.chain_forward(f.astype(np.complex128), pad[0], pad[1], wl, dist, 3.74e-6, aperture_radius=19200)
+    assert rel_l2(V, Vo) < 2e-5
+    gV = (rng.normal(size=V.shape) + 1j * rng.normal(size=V.shape)).astype(np.complex64)
+    gf = plan.backward(torch.from_numpy(f).cuda(), torch.from_numpy(gV).cuda()).cpu().numpy()
+    go = ob.chain_backward(f.astype(np.complex128), gV.astype(np.complex128), pad[0], pad[1], wl, dist, 3.74e-6,
+                           aperture_radius=19200)
+    assert rel_l2(gf, go) < 2e-5

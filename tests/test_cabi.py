@@ -41,3 +41,25 @@ def test_host_only_queries():
     assert lib.cvqpg_render_num_lists(2, 1920, 1080) == 1
     with pytest.raises(RuntimeError):
         _lib.size_query(lib.cvqpg_render_workspace_size, -1, 64, 64, 10)
+
+
+def test_blasm_host_queries():
+    import ctypes as ct
+    from complex_valued_quadratic_phase_gaussian_b200 import _lib
+    from complex_valued_quadratic_phase_gaussian_b200.propagator import BlasmParams
+    lib = _lib.lib()
+    p = BlasmParams()
+    p.channels, p.planes, p.height, p.width, p.pad_height, p.pad_width = 3, 3, 1080, 1920, 1408, 2240
+    p.pixel_pitch = 3.74e-6
+    for i, wl in enumerate((639e-9, 515e-9, 473e-9)):
+        p.wavelengths[i] = wl
+    for i, z in enumerate((5e-4, 1e-3, 1.5e-3)):
+        p.distances[i] = z
+    t = _lib.size_query(lib.cvqpg_blasm_tables_size, ct.byref(p))
+    w = _lib.size_query(lib.cvqpg_blasm_workspace_size, ct.byref(p))
+    assert 0 < t < 1 << 20
+    # row-pass intermediate (C x 2pW x pH) + kept column output (P x C x H x 2pW), complex64
+    assert w >= 8 * (3 * 4480 * 1408 + 9 * 1080 * 4480)
+    p.height = 1081  # odd sizes are rejected
+    with pytest.raises(RuntimeError):
+        _lib.size_query(lib.cvqpg_blasm_workspace_size, ct.byref(p))
