@@ -192,7 +192,8 @@ __global__ void __launch_bounds__(kColThreads, 1) blasm_cols_fwd_kernel(BlasmDev
 // K3: inverse FFT of a kept row (first pass reads global), keep out_w columns
 // -> V [P*C][out_h][out_w]
 __global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_kernel(BlasmDev d, const float2* __restrict__ B,
-                                                                     float2* __restrict__ V) {
+                                                                     float2* __restrict__ V,
+                                                                     float* __restrict__ pred) {
     extern __shared__ float2 sm[];
     const int ld = fft_ld(d.NW);
     const size_t row = blockIdx.x;  // pc * out_h + y
@@ -200,7 +201,17 @@ __global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_kernel(BlasmDev d,
     float2* res = fft_run([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, 0, d.row, true);
     const int col0 = (d.NW >> 1) - (d.out_w >> 1);
     float2* dst = V + row * d.out_w;
-    for (int x = threadIdx.x; x < d.out_w; x += blockDim.x) dst[x] = res[fft_pad(col0 + x)];
+    if (pred) {
+        // also the training prediction clamp(|V|^2, 0, 1) (train_2d_gaussian_rgb.py:193-194)
+        float* pd = pred + row * d.out_w;
+        for (int x = threadIdx.x; x < d.out_w; x += blockDim.x) {
+            const float2 v = res[fft_pad(col0 + x)];
+            dst[x] = v;
+            pd[x] = fminf(v.x * v.x + v.y * v.y, 1.0f);
+        }
+    } else {
+        for (int x = threadIdx.x; x < d.out_w; x += blockDim.x) dst[x] = res[fft_pad(col0 + x)];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -209,6 +220,8 @@ __global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_kernel(BlasmDev d,
 // K3b: gradient row embedded at the out_w centred columns -> forward FFT ->
 // tiled [P*C][NW/G][out_h][G]
 __global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_adj_kernel(BlasmDev d, const float2* __restrict__ gV,
+                                                                         const float* __restrict__ gpred,
+                                                                         const float2* __restrict__ Vf,
                                                                          float2* __restrict__ Bt) {
     extern __shared__ float2 sm[];
     const int ld = fft_ld(d.NW);
@@ -216,13 +229,29 @@ __global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_adj_kernel(BlasmDe
     const int pc = row / d.out_h, y = row - pc * d.out_h;
     const int col0 = (d.NW >> 1) - (d.out_w >> 1);
     const int ow = d.out_w;
-    const float2* src = gV + (size_t)row * ow;
-    float2* res = fft_run(
-        [=](int, int e) {
-            const int x = e - col0;
-            return (x < 0 || x >= ow) ? make_float2(0.f, 0.f) : __ldg(&src[x]);
-        },
-        sm, sm + ld, ld, 0, d.row, false);
+    float2* res;
+    if (gpred) {
+        // dL/dV = 2 V dL/dpred where 0 <= |V|^2 <= 1 (clamp passes its bounds), else 0
+        const float* gp = gpred + (size_t)row * ow;
+        const float2* vv = Vf + (size_t)row * ow;
+        res = fft_run(
+            [=](int, int e) {
+                const int x = e - col0;
+                if (x < 0 || x >= ow) return make_float2(0.f, 0.f);
+                const float2 v = __ldg(&vv[x]);
+                const float g = (v.x * v.x + v.y * v.y <= 1.0f) ? 2.0f * __ldg(&gp[x]) : 0.0f;
+                return make_float2(g * v.x, g * v.y);
+            },
+            sm, sm + ld, ld, 0, d.row, false);
+    } else {
+        const float2* src = gV + (size_t)row * ow;
+        res = fft_run(
+            [=](int, int e) {
+                const int x = e - col0;
+                return (x < 0 || x >= ow) ? make_float2(0.f, 0.f) : __ldg(&src[x]);
+            },
+            sm, sm + ld, ld, 0, d.row, false);
+    }
     const int G = d.G, ngroups = d.NW / G;
     for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) {
         const int gi = kx / G, g = kx - gi * G;
@@ -467,7 +496,7 @@ static void dispatch_cols_adj(const BlasmDev& d, const float2* Bt, float2* Ab, c
     else launch_cols_adj<G, 32>(d, Bt, Ab, s);
 }
 
-void blasm_forward(const BlasmDev& d, const float2* in, float2* out, void* workspace, cudaStream_t s) {
+void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace, cudaStream_t s) {
     float2 *A, *B;
     carve(d, workspace, &A, &B);
     const size_t rs = row_smem(d);
@@ -477,16 +506,16 @@ void blasm_forward(const BlasmDev& d, const float2* in, float2* out, void* works
     else if (d.G == 2) launch_cols_fwd<2>(d, A, B, s);
     else launch_cols_fwd<1>(d, A, B, s);
     CVQPG_SMEM_ATTR(blasm_rows_inv_kernel, rs);
-    blasm_rows_inv_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, B, out);
+    blasm_rows_inv_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, B, out, pred);
 }
 
-void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* grad_out, float2* grad_in,
-                    void* workspace, cudaStream_t s) {
+void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* grad_out, const float* grad_pred,
+                    const float2* vfield, float2* grad_in, void* workspace, cudaStream_t s) {
     float2 *A, *B;
     carve(d, workspace, &A, &B);
     const size_t rs = row_smem(d);
     CVQPG_SMEM_ATTR(blasm_rows_fwd_adj_kernel, rs);
-    blasm_rows_fwd_adj_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, grad_out, B);
+    blasm_rows_fwd_adj_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, grad_out, grad_pred, vfield, B);
     if (d.G == 4) dispatch_cols_adj<4>(d, B, A, s);
     else if (d.G == 2) dispatch_cols_adj<2>(d, B, A, s);
     else dispatch_cols_adj<1>(d, B, A, s);
@@ -610,7 +639,7 @@ extern "C" int cvqpg_blasm_forward(const cvqpg_blasm_params* p, const void* tabl
     if (!fits(d)) return CVQPG_ERR_UNSUPPORTED;
     if (!input || !out_field || !workspace) return CVQPG_ERR_ARG;
     if (workspace_bytes < blasm_workspace_bytes(d)) return CVQPG_ERR_WORKSPACE;
-    blasm_forward(d, (const float2*)input, (float2*)out_field, workspace, (cudaStream_t)stream);
+    blasm_forward(d, (const float2*)input, (float2*)out_field, nullptr, workspace, (cudaStream_t)stream);
     return launch_status();
 }
 
@@ -623,7 +652,7 @@ extern "C" int cvqpg_blasm_backward(const cvqpg_blasm_params* p, const void* tab
     if (!fits(d)) return CVQPG_ERR_UNSUPPORTED;
     if (!grad_out || !grad_input || !workspace || (d.input_mode == 0 && !input)) return CVQPG_ERR_ARG;
     if (workspace_bytes < blasm_workspace_bytes(d)) return CVQPG_ERR_WORKSPACE;
-    blasm_backward(d, (const float2*)input, (const float2*)grad_out, (float2*)grad_input, workspace,
-                   (cudaStream_t)stream);
+    blasm_backward(d, (const float2*)input, (const float2*)grad_out, nullptr, nullptr, (float2*)grad_input,
+                   workspace, (cudaStream_t)stream);
     return launch_status();
 }

@@ -44,8 +44,11 @@ int blasm_make_dev(const cvqpg_blasm_params* prm, const void* tables, size_t tab
 
 size_t blasm_workspace_bytes(const BlasmDev& d);
 
-void blasm_forward(const BlasmDev& d, const float2* in, float2* out, void* workspace, cudaStream_t stream);
-void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* grad_out, float2* grad_in,
-                    void* workspace, cudaStream_t stream);
+// pred (nullable): also write clamp(|V|^2, 0, 1) [P*C][out_h][out_w].
+void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace,
+                   cudaStream_t stream);
+// Either grad_out = dL/dV, or (grad_pred = dL/dpred, vfield = V) with dL/dV formed on load.
+void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* grad_out, const float* grad_pred,
+                    const float2* vfield, float2* grad_in, void* workspace, cudaStream_t stream);
 
 }  // namespace cvqpg

@@ -186,6 +186,116 @@ CVQPG_API int cvqpg_blasm_backward(const cvqpg_blasm_params* prm, const void* ta
                                    const float* input, const float* grad_out, float* grad_input,
                                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- fused multi-plane loss ---------------------------------------------
+ *
+ * Replaces, per plane p of the fit loop (train_2d_gaussian_rgb.py:192-199),
+ *   multiplane_loss_odak.__call__(pred, target, p, inject_noise=True)
+ *                                       (utils/propagator.py:417-449)
+ *   + GaussianLoss(pred, target)        (utils/data_utils.py:22-41)
+ * for all planes in one launch, with pred = clamp(|V_p|^2, 0, 1):
+ *   L = sum_p  w_l2 mean((pred-T)^2) + w_mask mean((pred M - N M)^2)
+ *            + w_cor mean((pred N - N N)^2) + ssim_weight (1 - SSIM(pred, T))
+ * M = [depth_plane == p]; N = T + (z * noise_ratio) * target_range[p] with a
+ * fresh standard normal z per element and iteration (Philox4x32-10 keyed by
+ * `seed`, counter = (element, *iteration)); SSIM with the pytorch_msssim
+ * defaults (11-tap Gaussian, sigma 1.5, K = 0.01/0.03, data range 1, valid).
+ * Writes grad_pred = dL/dpred [P,C,H,W] and out[1 + 3P]:
+ *   out[0] loss, out[1+p] MSE(pred_p, T_p) (PSNR = -10 log10 MSE),
+ *   out[1+P+p] SSIM_p, out[1+2P+p] loss of plane p.
+ */
+typedef struct cvqpg_loss_params {
+    int channels;
+    int planes;
+    int height, width;
+    float w_l2, w_mask, w_cor;  /* reference weights [1, 1, 1] (utils/data_utils.py:75) */
+    float ssim_weight;          /* reference 0.025 * 0.2 = 0.005 (utils/data_utils.py:22-41) */
+    float noise_ratio;          /* reference 1e-3 (utils/propagator.py:417) */
+    int inject_noise;           /* 1 in the fit loop (train_2d_gaussian_rgb.py:195) */
+    unsigned long long seed;
+} cvqpg_loss_params;
+
+CVQPG_API int cvqpg_loss_workspace_size(const cvqpg_loss_params* prm, size_t* bytes);
+/* target_range[p] = max(T_p) - min(T_p), once per fit (targets are constant). */
+CVQPG_API int cvqpg_loss_target_range(const float* targets, int planes, int channels, int height, int width,
+                                      float* target_range, void* stream);
+CVQPG_API int cvqpg_loss_forward_backward(const cvqpg_loss_params* prm, const float* pred, const float* targets,
+                                          const uint8_t* depth_plane, const float* target_range,
+                                          const int32_t* iteration, float* grad_pred, float* out,
+                                          void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- fused fit iteration ---------------------------------------------------
+ *
+ * One call = one iteration of the reference fit loop body
+ * (train_2d_gaussian_rgb.py:187-211): render (preprocess, bin, splat) ->
+ * pad/clamp + BLASM to every plane -> multi-plane loss + SSIM -> adjoint of
+ * all of it -> nan_to_num -> clip_grad_norm_(max_grad_norm) -> Adan step,
+ * plus the means cosine schedule and the curvature warm-up. Every stage is a
+ * kernel on `stream`; nothing synchronises the host, so the call can be
+ * captured once in a CUDA graph and replayed. The iteration counter lives in
+ * device memory (`iteration`, incremented at the end of each step) and drives
+ * the learning-rate table, the warm-up and the per-iteration target noise.
+ *
+ * Parameter layout (one flat float buffer, reference tensor order and shapes,
+ * model_2d_gaussian_rgb.py:18-26), with N = num_gaussians, C = channels:
+ *   means_2d [N,2] | pre_act_scales [N,2] | pre_act_rotation [N] | colours [N,C]
+ *   | pre_act_phase [N,C] | pre_act_opacities [N] | curvature [N]
+ * `grads` has the same layout; `adan_state` holds exp_avg, exp_avg_sq,
+ * exp_avg_diff, neg_pre_grad, each in that layout (utils/optimizer.py:161-169).
+ * Param groups (train_2d_gaussian_rgb.py:73-86): lr[0] means (optionally a
+ * per-iteration table), lr[1] scales, lr[2] colours + phase, lr[3] opacities,
+ * lr[4] rotation, lr[5] curvature.
+ * history: ring of history_len records of 1 + 3P floats (cvqpg_loss_forward_backward
+ * `out` layout), record (iteration % history_len) written each step.
+ * status[0] is set to 1 (and stays) if a step's tile pairs exceeded pair_capacity.
+ */
+typedef struct cvqpg_fit_params {
+    int channels, planes;
+    int height, width;
+    int pad_height, pad_width;
+    int num_gaussians;
+    int pair_capacity;
+    int cull_mode;          /* CVQPG_CULL_*; the CUDA renderer's rule by default */
+    int curv_mode;          /* 0 off ('flat'), 1 constant, 2 scale_aware */
+    int curv_trainable;     /* 0 for --primitive flat */
+    int warmup_iters;       /* curvature frozen for the first warmup_iters iterations */
+    int num_iters;          /* length of the means learning-rate table */
+    int history_len;
+    int no_prox;
+    int inject_noise;
+    double pixel_pitch;
+    double wavelengths[3];
+    double distances[8];
+    double aperture_radius;
+    double curv_nyquist;    /* 0.9 */
+    double curv_const;      /* 200 */
+    double lr[6];
+    double betas[3];        /* (0.98, 0.92, 0.99) */
+    double eps;             /* 1e-8 */
+    double weight_decay;    /* 0 */
+    double max_grad_norm;   /* 1.0 */
+    float loss_weights[3];  /* [1, 1, 1] */
+    float ssim_weight;      /* 0.005 */
+    float noise_ratio;      /* 1e-3 */
+    float reserved;
+    unsigned long long seed;
+} cvqpg_fit_params;
+
+CVQPG_API int cvqpg_fit_workspace_size(const cvqpg_fit_params* prm, size_t* bytes);
+/* Synchronous: fills the workspace's constant tables (BLASM tables, lr table of
+ * num_iters doubles for the means group, or NULL for a constant lr[0]). */
+CVQPG_API int cvqpg_fit_setup(const cvqpg_fit_params* prm, const double* means_lr_table, void* workspace,
+                              size_t workspace_bytes);
+CVQPG_API int cvqpg_fit_step(const cvqpg_fit_params* prm, float* params, float* grads, float* adan_state,
+                             const float* targets, const uint8_t* depth_plane, const float* target_range,
+                             int32_t* iteration, float* history, int32_t* status, void* workspace,
+                             size_t workspace_bytes, void* stream);
+/* Forward only (no noise, no update): out = 1 + 3P floats as in the loss; optionally
+ * the splat field [C,H,W] and the plane fields V [P,C,H,W] (complex64) when non-null. */
+CVQPG_API int cvqpg_fit_evaluate(const cvqpg_fit_params* prm, const float* params, const float* targets,
+                                 const uint8_t* depth_plane, const float* target_range, float* out,
+                                 float* field_out, float* planes_out, int32_t* status, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -263,6 +263,109 @@ def golden_propagate(C, name, seed, H, W, pH, pW, P, d_val, vd, aperture_size):
                         I_crop=I_crop.detach().numpy(), wts=wts.numpy(), grad_field=f.grad.numpy())
 
 
+class _MeansCosine:
+    """The training script's MeansCosineScheduler (train_2d_gaussian_rgb.py:58-70), restated as glue
+    because the script itself imports packages that are not installed here."""
+
+    def __init__(self, optimizer, num_itrs, eta_min=1e-3):
+        self.optimizer = optimizer
+        self.group_indices = [i for i, g in enumerate(optimizer.param_groups) if g.get("name") == "means"]
+        tmp = torch.optim.SGD([{"params": optimizer.param_groups[i]["params"], "lr": optimizer.param_groups[i]["lr"]}
+                               for i in self.group_indices])
+        self.sch = torch.optim.lr_scheduler.CosineAnnealingLR(tmp, T_max=max(1, num_itrs), eta_min=eta_min)
+
+    def step(self):
+        self.sch.step()
+        for i, gi in enumerate(self.group_indices):
+            self.optimizer.param_groups[gi]["lr"] = self.sch.get_last_lr()[i]
+
+
+def golden_fit(C, name, seed, W=96, H=64, N=200, P=2, pad=(96, 128), iters=3, warmup=1, num_itrs=10,
+               d_val=1e-3, vd=1e-3):
+    """Iterations of the reference fit loop body (train_2d_gaussian_rgb.py:179-211) on the torch renderer."""
+    from oracle import loss as oloss
+    from complex_valued_quadratic_phase_gaussian_b200 import scenes as sc
+    model = load_by_path(f"ref_model_{C}", ref("model_2d_gaussian_rgb.py" if C == 3 else
+                                              "model_2d_gaussian_grayscale.py"))
+    prop_mod = load_by_path("ref_propagator", ref("utils/propagator.py"))
+    opt_mod = load_by_path("ref_optimizer", ref("utils/optimizer.py"))
+    du = load_by_path("ref_data_utils", ref("utils/data_utils.py"))
+    import odak
+    torch.manual_seed(seed)
+    if C == 3:
+        img, depth = sc.rgb_blobs(H, W, seed=seed, num_blobs=40)
+    else:
+        img, depth = sc.grayscale_blobs(H, W, seed=seed, num_blobs=12)
+    wl = WAVELENGTHS if C == 3 else WAVELENGTHS[:1]
+    ap = _args_prop(C, pad)
+    ap.num_planes, ap.split_ratio = P, 1.0
+    distances = torch.linspace(-vd / 2.0, vd / 2.0, P) + d_val
+    prop = prop_mod.propagator(resolution=list(pad), wavelengths=wl, pixel_pitch=PITCH, number_of_frames=C,
+                               distances=distances, propagation_type="Bandlimited Angular Spectrum",
+                               laser_channel_power=torch.eye(C), aperture_size=10 * max(W, H), device="cpu")
+    loss_fn = prop_mod.multiplane_loss_odak(target_image=torch.from_numpy(img), target_depth=torch.from_numpy(depth)[None],
+                                            target_blur_size=20, number_of_planes=P, blur_ratio=8,
+                                            weights=[1.0, 1.0, 1.0, 0.0], scheme="defocus", reduction="mean",
+                                            split_ratio=1.0, device="cpu")
+    targets, masks, qdepth = loss_fn.get_targets()
+    rng = np.random.default_rng(seed)
+    raw = raw_params(rng, N, W, H, C, curv_scale=1.0)
+    raw["pre_act_phase"] = rng.uniform(0, 2 * np.pi, (N, C)).astype(np.float32)
+    g = _make_gaussians(model, raw, W, H, C, ap, "scale_aware")
+    scene = model.Scene2D(g, ap)
+    g.curvature.requires_grad_(False)
+    groups = [{"params": [g.means_2d], "lr": 0.01, "name": "means"},
+              {"params": [g.pre_act_scales], "lr": 0.005, "name": "scales"},
+              {"params": [g.colours, g.pre_act_phase], "lr": 0.0025, "name": "amplitude_phase"},
+              {"params": [g.pre_act_opacities], "lr": 0.025, "name": "opacity"},
+              {"params": [g.pre_act_rotation], "lr": 0.001, "name": "rotation"},
+              {"params": [g.curvature], "lr": 0.001, "name": "curvature"}]
+    opt = opt_mod.Adan(groups, lr=0, eps=1e-8, foreach=False)
+    sched = _MeansCosine(opt, num_itrs)
+    trainable = [p for gr in groups for p in gr["params"]]
+    rec = {"loss": [], "mse0": []}
+    noise_seed = seed
+    real_randn_like = torch.randn_like
+    for itr in range(iters):
+        if itr == warmup:
+            g.curvature.requires_grad_(True)
+        opt.zero_grad()
+        holo = scene.render((W, H))
+        phase_map = odak.learn.wave.calculate_phase(holo) % (2 * odak.pi)
+        amp = torch.clamp(odak.learn.wave.calculate_amplitude(holo), min=0.0, max=1.0)
+        recon = prop.reconstruct(phase_map, amplitude=amp, no_grad=False).sum(0)
+        noise = torch.from_numpy(oloss.plane_noise((P, C, H, W), noise_seed, itr))
+        loss = 0.0
+        for idx, (ri, tgt) in enumerate(zip(recon, targets)):
+            pred = torch.clamp(odak.learn.tools.crop_center(ri, size=(H, W)), min=0.0, max=1.0)
+            torch.randn_like = lambda t, _n=noise[idx]: _n.clone()
+            try:
+                loss = loss + loss_fn(pred, tgt, idx, inject_noise=True)
+            finally:
+                torch.randn_like = real_randn_like
+            loss = loss + (du.GaussianLoss(pred, tgt) if C == 3 else du.GaussianLossGrayscale(pred, tgt))
+            if idx == 0:
+                rec["mse0"].append(float(((pred - tgt) ** 2).mean()))
+        rec["loss"].append(float(loss))
+        loss.backward()
+        for p_ in trainable:
+            if p_.grad is not None:
+                p_.grad = torch.nan_to_num(p_.grad, nan=0.0, posinf=0.0, neginf=0.0)
+        torch.nn.utils.clip_grad_norm_(trainable, max_norm=1.0)
+        opt.step()
+        sched.step()
+        for k in RAW_KEYS:
+            rec.setdefault(f"it{itr}_{k}", getattr(g, k).detach().numpy().copy())
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), W=W, H=H, C=C, N=N, P=P, pad=np.array(pad),
+                        distances=distances.double().numpy(), wavelengths=np.array(wl), pitch=PITCH, seed=noise_seed,
+                        warmup=warmup, num_itrs=num_itrs, iters=iters, aperture=10 * max(W, H),
+                        targets=targets.numpy(),
+                        depth_plane=loss_fn.target_depth.numpy().astype(np.uint8).reshape(H, W),  # plane index
+                        loss=np.array(rec["loss"]), mse0=np.array(rec["mse0"]),
+                        **{f"init_{k}": v for k, v in raw.items()},
+                        **{k: v for k, v in rec.items() if k.startswith("it")})
+
+
 GOLDENS = {
     "splat_rgb": lambda: golden_splat(3, "splat_rgb", 11),
     "splat_gray": lambda: golden_splat(1, "splat_gray", 12),
@@ -275,6 +378,8 @@ GOLDENS = {
     # 2pH = 2pW = 120 = 8*3*5: band limit active (z = 5 cm) and a small Fourier aperture
     "propagate_gray_bandlimit": lambda: golden_propagate(1, "propagate_gray_bandlimit", 42, 32, 32, 60, 60, 2,
                                                          5e-2, 2e-2, 40),
+    "fit_rgb": lambda: golden_fit(3, "fit_rgb", 51),
+    "fit_gray": lambda: golden_fit(1, "fit_gray", 52, P=3),
 }
 
 
