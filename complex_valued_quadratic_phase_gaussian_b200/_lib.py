@@ -46,6 +46,7 @@ _SIGNATURES = {
     "cvqpg_fit_workspace_size": [_p, _psz],
     "cvqpg_fit_setup": [_p, _p, _p, _sz],
     "cvqpg_fit_step": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
+    "cvqpg_fit_step_timed": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p, _i],
     "cvqpg_fit_evaluate": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
 }
 _RESTYPES = {"cvqpg_status_string": ctypes.c_char_p}

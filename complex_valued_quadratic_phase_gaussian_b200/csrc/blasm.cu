@@ -496,32 +496,39 @@ static void dispatch_cols_adj(const BlasmDev& d, const float2* Bt, float2* Ab, c
     else launch_cols_adj<G, 32>(d, Bt, Ab, s);
 }
 
-void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace, cudaStream_t s) {
+void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace, cudaStream_t s,
+                   StageMarks* marks) {
     float2 *A, *B;
     carve(d, workspace, &A, &B);
     const size_t rs = row_smem(d);
     CVQPG_SMEM_ATTR(blasm_rows_fwd_kernel, rs);
     blasm_rows_fwd_kernel<<<d.C * d.pH, kRowThreads, rs, s>>>(d, in, A);
+    if (marks) marks->mark(s);
     if (d.G == 4) launch_cols_fwd<4>(d, A, B, s);
     else if (d.G == 2) launch_cols_fwd<2>(d, A, B, s);
     else launch_cols_fwd<1>(d, A, B, s);
+    if (marks) marks->mark(s);
     CVQPG_SMEM_ATTR(blasm_rows_inv_kernel, rs);
     blasm_rows_inv_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, B, out, pred);
+    if (marks) marks->mark(s);
 }
 
 void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* grad_out, const float* grad_pred,
-                    const float2* vfield, float2* grad_in, void* workspace, cudaStream_t s) {
+                    const float2* vfield, float2* grad_in, void* workspace, cudaStream_t s, StageMarks* marks) {
     float2 *A, *B;
     carve(d, workspace, &A, &B);
     const size_t rs = row_smem(d);
     CVQPG_SMEM_ATTR(blasm_rows_fwd_adj_kernel, rs);
     blasm_rows_fwd_adj_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, grad_out, grad_pred, vfield, B);
+    if (marks) marks->mark(s);
     if (d.G == 4) dispatch_cols_adj<4>(d, B, A, s);
     else if (d.G == 2) dispatch_cols_adj<2>(d, B, A, s);
     else dispatch_cols_adj<1>(d, B, A, s);
+    if (marks) marks->mark(s);
     const int in_h = d.input_mode == 0 ? d.H : d.pH;
     CVQPG_SMEM_ATTR(blasm_rows_inv_adj_kernel, rs);
     blasm_rows_inv_adj_kernel<<<d.C * in_h, kRowThreads, rs, s>>>(d, A, in_field, grad_in);
+    if (marks) marks->mark(s);
 }
 
 static bool fits(const BlasmDev& d) {

@@ -44,11 +44,22 @@ int blasm_make_dev(const cvqpg_blasm_params* prm, const void* tables, size_t tab
 
 size_t blasm_workspace_bytes(const BlasmDev& d);
 
+// Optional CUDA-event marks between kernels (bench-time stage timing).
+struct StageMarks {
+    cudaEvent_t* ev = nullptr;
+    int n = 0;
+    int idx = 0;
+    void mark(cudaStream_t s) {
+        if (ev && idx < n) cudaEventRecord(ev[idx++], s);
+    }
+};
+
 // pred (nullable): also write clamp(|V|^2, 0, 1) [P*C][out_h][out_w].
 void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace,
-                   cudaStream_t stream);
+                   cudaStream_t stream, StageMarks* marks = nullptr);
 // Either grad_out = dL/dV, or (grad_pred = dL/dpred, vfield = V) with dL/dV formed on load.
 void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* grad_out, const float* grad_pred,
-                    const float2* vfield, float2* grad_in, void* workspace, cudaStream_t stream);
+                    const float2* vfield, float2* grad_in, void* workspace, cudaStream_t stream,
+                    StageMarks* marks = nullptr);
 
 }  // namespace cvqpg

@@ -172,17 +172,22 @@ __global__ void record_step_kernel(const float* __restrict__ loss_out, int nvals
 // forward half shared by step and evaluate
 static void run_forward(const cvqpg_fit_params* q, const FitLayout& L, const BlasmDev& bd, const LossDev& ld,
                         const RawParams& raw, const float* targets, const uint8_t* depth_plane,
-                        const float* target_range, const int32_t* iteration, cudaStream_t s) {
-    const int N = q->num_gaussians, C = q->channels;
+                        const float* target_range, const int32_t* iteration, cudaStream_t s,
+                        StageMarks* marks = nullptr) {
+    const int C = q->channels;
     const PreDev P = make_pre(q);
     const BinRule rule = make_bin_rule(q->cull_mode, q->width, q->height, L.radii, L.radius3);
+    if (marks) marks->mark(s);
     launch_preprocess_forward(C, P, raw, L.records, L.radii, L.radius3, L.bin.tiles_touched, rule, s);
-    (void)N;
+    if (marks) marks->mark(s);
     launch_binning(rule, L.records, L.bin, L.point_list, L.ranges, L.pair_count, s);
+    if (marks) marks->mark(s);
     const float dxy2 = (float)(q->pixel_pitch * q->pixel_pitch);
     launch_splat_forward(C, rule, L.ranges, L.point_list, L.records, L.kvec, dxy2, L.field, s);
-    blasm_forward(bd, L.field, L.vfield, L.pred, L.blasm_ws, s);
+    if (marks) marks->mark(s);
+    blasm_forward(bd, L.field, L.vfield, L.pred, L.blasm_ws, s, marks);
     launch_loss(ld, L.pred, targets, depth_plane, target_range, iteration, L.gpred, L.loss_partials, L.loss_out, s);
+    if (marks) marks->mark(s);
 }
 
 }  // namespace cvqpg
@@ -231,10 +236,10 @@ static int fit_prepare(const cvqpg_fit_params* q, void* workspace, size_t bytes,
     return fit_layout(q, workspace, bytes, L, bd, ld);
 }
 
-extern "C" int cvqpg_fit_step(const cvqpg_fit_params* q, float* params, float* grads, float* adan_state,
-                              const float* targets, const uint8_t* depth_plane, const float* target_range,
-                              int32_t* iteration, float* history, int32_t* status, void* workspace, size_t bytes,
-                              void* stream_) {
+static int fit_step_impl(const cvqpg_fit_params* q, float* params, float* grads, float* adan_state,
+                         const float* targets, const uint8_t* depth_plane, const float* target_range,
+                         int32_t* iteration, float* history, int32_t* status, void* workspace, size_t bytes,
+                         void* stream_, StageMarks* marks) {
     FitLayout L;
     BlasmDev bd;
     LossDev ld;
@@ -246,11 +251,11 @@ extern "C" int cvqpg_fit_step(const cvqpg_fit_params* q, float* params, float* g
     const int N = q->num_gaussians, C = q->channels, P = q->planes;
     FlatViews fv = flat_views(q, params, grads);
     // forward: render, propagate, loss (+ dL/dpred)
-    run_forward(q, L, bd, ld, fv.raw, targets, depth_plane, target_range, iteration, s);
+    run_forward(q, L, bd, ld, fv.raw, targets, depth_plane, target_range, iteration, s, marks);
     record_step_kernel<<<1, 64, 0, s>>>(L.loss_out, 1 + 3 * P, L.pair_count, history, q->history_len, status,
                                         iteration, 0);
     // adjoint of the propagation (dL/dpred -> dL/dU)
-    blasm_backward(bd, L.field, nullptr, L.gpred, L.vfield, L.gfield, L.blasm_ws, s);
+    blasm_backward(bd, L.field, nullptr, L.gpred, L.vfield, L.gfield, L.blasm_ws, s, marks);
     // splat adjoint
     cudaMemsetAsync(L.splat_grads, 0, sizeof(float) * (size_t)(8 + 2 * C) * (N > 0 ? N : 1), s);
     float* sg = L.splat_grads;
@@ -259,9 +264,11 @@ extern "C" int cvqpg_fit_step(const cvqpg_fit_params* q, float* params, float* g
     const BinRule rule = make_bin_rule(q->cull_mode, q->width, q->height, L.radii, L.radius3);
     const float dxy2 = (float)(q->pixel_pitch * q->pixel_pitch);
     launch_splat_backward(C, rule, L.ranges, L.point_list, L.records, L.kvec, dxy2, L.gfield, out, s);
+    if (marks) marks->mark(s);
     // preprocessing adjoint + nan_to_num + norm partials
     SplatGradsIn gin{out.d_means, out.d_inv, out.d_col, out.d_ph, out.d_op, out.d_cv, out.d_ar};
     launch_preprocess_backward(C, make_pre(q), fv.raw, gin, fv.grads, iteration, L.norm_partials, s);
+    if (marks) marks->mark(s);
     // clip + Adan
     AdanDev A;
     std::memset(&A, 0, sizeof(A));
@@ -296,8 +303,28 @@ extern "C" int cvqpg_fit_step(const cvqpg_fit_params* q, float* params, float* g
     A.norm_partials = L.norm_partials;
     A.num_partials = preprocess_backward_blocks(N);
     if (N > 0) launch_adan(A, iteration, s);
+    if (marks) marks->mark(s);
     record_step_kernel<<<1, 32, 0, s>>>(L.loss_out, 0, L.pair_count, nullptr, 1, nullptr, iteration, 1);
     return launch_status();
+}
+
+extern "C" int cvqpg_fit_step(const cvqpg_fit_params* q, float* params, float* grads, float* adan_state,
+                              const float* targets, const uint8_t* depth_plane, const float* target_range,
+                              int32_t* iteration, float* history, int32_t* status, void* workspace, size_t bytes,
+                              void* stream) {
+    return fit_step_impl(q, params, grads, adan_state, targets, depth_plane, target_range, iteration, history, status,
+                         workspace, bytes, stream, nullptr);
+}
+
+extern "C" int cvqpg_fit_step_timed(const cvqpg_fit_params* q, float* params, float* grads, float* adan_state,
+                                    const float* targets, const uint8_t* depth_plane, const float* target_range,
+                                    int32_t* iteration, float* history, int32_t* status, void* workspace,
+                                    size_t bytes, void* stream, void** stage_events, int num_events) {
+    StageMarks m;
+    m.ev = (cudaEvent_t*)stage_events;
+    m.n = num_events;
+    return fit_step_impl(q, params, grads, adan_state, targets, depth_plane, target_range, iteration, history, status,
+                         workspace, bytes, stream, &m);
 }
 
 extern "C" int cvqpg_fit_evaluate(const cvqpg_fit_params* q, const float* params, const float* targets,

@@ -270,6 +270,27 @@ class Fitter:
             _lib.ptr(self.history), _lib.ptr(self.status), _lib.ptr(self.workspace), self.ws_bytes,
             ctypes.c_void_p(stream))
 
+    STAGES = ("preprocess", "binning", "splat", "blasm_rows", "blasm_columns", "blasm_inverse_rows", "loss",
+              "adjoint_rows", "adjoint_columns", "adjoint_inverse_rows", "splat_adjoint", "preprocess_adjoint",
+              "clip_adan")
+
+    def step_timed(self):
+        """One eager iteration with CUDA events at the stage boundaries; returns {stage: ms} after a sync."""
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(self.STAGES) + 1)]
+        s = torch.cuda.current_stream(self.device)
+        for e in evs:  # materialise the event handles
+            e.record(s)
+        arr = (ctypes.c_void_p * len(evs))(*[ctypes.c_void_p(e.cuda_event) for e in evs])
+        p = self.params
+        st = self._lib.cvqpg_fit_step_timed(
+            ctypes.byref(p), _lib.ptr(self.flat), _lib.ptr(self.grads), _lib.ptr(self.adan_state),
+            _lib.ptr(self.targets), _lib.ptr(self.depth_plane), _lib.ptr(self.target_range), _lib.ptr(self.iteration),
+            _lib.ptr(self.history), _lib.ptr(self.status), _lib.ptr(self.workspace), self.ws_bytes,
+            ctypes.c_void_p(s.cuda_stream), arr, len(evs))
+        _lib.check(st, "cvqpg_fit_step_timed")
+        torch.cuda.synchronize(self.device)
+        return {name: evs[i].elapsed_time(evs[i + 1]) for i, name in enumerate(self.STAGES)}
+
     def step(self):
         """One fit iteration (eager launches on the current stream)."""
         s = torch.cuda.current_stream(self.device).cuda_stream
@@ -279,7 +300,10 @@ class Fitter:
         """Record one iteration into a CUDA graph (the iteration state is in device memory)."""
         self.step()  # warm kernels / lazy attribute setup outside capture
         torch.cuda.synchronize(self.device)
-        g = torch.cuda.CUDAGraph()
+        try:
+            g = torch.cuda.CUDAGraph(keep_graph=True)  # keep the cudaGraph_t for node inspection
+        except TypeError:
+            g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(self.device)
         s.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(s):

@@ -289,6 +289,16 @@ CVQPG_API int cvqpg_fit_step(const cvqpg_fit_params* prm, float* params, float* 
                              const float* targets, const uint8_t* depth_plane, const float* target_range,
                              int32_t* iteration, float* history, int32_t* status, void* workspace,
                              size_t workspace_bytes, void* stream);
+/* cvqpg_fit_step with CUDA events recorded on `stream` at the stage
+ * boundaries (for timing; not for graph capture). Stage order, 14 events:
+ *  0 start | 1 preprocess | 2 binning | 3 splat | 4 BLASM rows | 5 BLASM columns
+ *  6 BLASM inverse rows | 7 loss | 8 adjoint rows | 9 adjoint columns
+ * 10 adjoint inverse rows | 11 splat adjoint | 12 preprocess adjoint | 13 clip + Adan
+ * (event i marks the end of the stage named at i; event 0 the start). */
+CVQPG_API int cvqpg_fit_step_timed(const cvqpg_fit_params* prm, float* params, float* grads, float* adan_state,
+                                   const float* targets, const uint8_t* depth_plane, const float* target_range,
+                                   int32_t* iteration, float* history, int32_t* status, void* workspace,
+                                   size_t workspace_bytes, void* stream, void** stage_events, int num_events);
 /* Forward only (no noise, no update): out = 1 + 3P floats as in the loss; optionally
  * the splat field [C,H,W] and the plane fields V [P,C,H,W] (complex64) when non-null. */
 CVQPG_API int cvqpg_fit_evaluate(const cvqpg_fit_params* prm, const float* params, const float* targets,
