@@ -28,6 +28,8 @@ _SIGNATURES = {
     "cvqpg_render_num_lists": [_i, _i, _i],
     "cvqpg_render_forward": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _f, _i, _i, _i, _i,
                              _p, _p, _i, _p, _p, _p, _sz, _p],
+    "cvqpg_render_forward_noalloc": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _f, _i, _i, _i, _i,
+                                     _p, _p, _i, _p, _p, _p],
     "cvqpg_render_forward_cull": [_p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _f, _i, _i, _i, _i,
                                   _p, _p, _i, _p, _p, _p, _sz, _p],
     "cvqpg_render_backward_workspace_size": [_i, _psz],

@@ -49,7 +49,7 @@ __global__ void pack_records_kernel(int n, const float* __restrict__ means, cons
     for (int q = 0; q < 4; q++) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
 }
 
-static void launch_pack_records(int channels, int n, const float* means, const float* inv_cov, const float* colours,
+void launch_pack_records(int channels, int n, const float* means, const float* inv_cov, const float* colours,
                                 const float* phase, const float* opac, const float* curv, const float* area,
                                 float* rec, cudaStream_t stream) {
     if (n <= 0) return;

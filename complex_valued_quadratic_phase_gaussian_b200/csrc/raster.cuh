@@ -52,6 +52,11 @@ struct BinRule {
 BinRule make_bin_rule(int mode, int width, int height, const int32_t* radii, const float* radius_f);
 inline int bin_rule_lists(const BinRule& r) { return r.lgx * r.lgy; }
 
+// Pack the reference SoA tensors into records (drop-in path).
+void launch_pack_records(int channels, int n, const float* means, const float* inv_cov, const float* colours,
+                         const float* phase, const float* opac, const float* curv, const float* area, float* rec,
+                         cudaStream_t stream);
+
 // Count kernel for the drop-in path (records already packed).
 void launch_tile_count(const BinRule& rule, const float* records, int n, uint32_t* tiles_touched,
                        cudaStream_t stream);

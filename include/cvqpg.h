@@ -83,6 +83,30 @@ CVQPG_API int cvqpg_render_forward(const float* means_2d, const float* inv_cov, 
                          float* out_field, int32_t* point_list, int pair_capacity, int32_t* ranges,
                          int32_t* pair_count, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free render forward. No counterpart in the reference: the
+ * reference allocates its scratch with torch on every call.
+ * Same inputs, outputs and status codes as cvqpg_render_forward, without the
+ * workspace argument, for callers that cannot allocate device memory where
+ * they render (a host that owns every allocation and passes only its own
+ * buffers, a process running under a fixed device-memory budget, or code that
+ * must not call cudaMalloc because it would synchronise the device). The
+ * scratch is a fixed device array inside the library (about 5.5 MiB, held by
+ * every GPU that loads the library until exit), so:
+ *   - n <= 16384 Gaussians and pair_capacity <= 262144, else CVQPG_ERR_UNSUPPORTED;
+ *   - the first call on a device looks the array up (cudaGetSymbolAddress) for
+ *     the device that is current; make that first call before any stream capture;
+ *   - all calls share the array: calls that can overlap on the GPU (different
+ *     streams, or different host threads) race and must be serialised;
+ *   - nothing in the array needs clearing between calls (every buffer is
+ *     written before it is read).
+ * It calls no cudaMalloc, cudaFree or allocating library routine. */
+CVQPG_API int cvqpg_render_forward_noalloc(const float* means_2d, const float* inv_cov, const float* colours,
+                                           const float* phase, const float* opacities, const float* curvature,
+                                           const float* area, const int32_t* radii, const float* k, float dxy2,
+                                           int n, int width, int height, int channels,
+                                           float* out_field, int32_t* point_list, int pair_capacity,
+                                           int32_t* ranges, int32_t* pair_count, void* stream);
+
 /* Number of tile lists (rows of `ranges`) a culling rule produces. */
 CVQPG_API int cvqpg_render_num_lists(int cull_mode, int width, int height);
 
