@@ -1,0 +1,92 @@
+"""Run and time single stages of the fit iteration at a workload's size.
+
+    python -m complex_valued_quadratic_phase_gaussian_b200.stagebench --stage blasm_fwd --workload rgb1080 --iters 3
+
+Stages: ``blasm_fwd`` (rows, columns, inverse rows), ``blasm_adj`` (the three
+adjoint passes), ``render`` (binning + splat forward of the drop-in path).
+Only the buffers of that stage are allocated, so the process stays small
+enough for kernel-level profiling. Prints one JSON line with the mean
+milliseconds per call (CUDA events on the launching stream).
+"""
+import argparse
+import json
+
+import numpy as np
+import torch
+
+from .propagator import BlasmPlan, reference_distances, reference_pad_size
+
+WORKLOADS = {
+    "rgb1080": dict(W=1920, H=1080, C=3, N=96000, P=3, wl=[639e-9, 515e-9, 473e-9], pitch=3.74e-6, d_val=1e-3,
+                    vd=1e-3),
+    "gray256": dict(W=256, H=256, C=1, N=4096, P=3, wl=[515e-9], pitch=8e-6, d_val=1.5e-3, vd=1e-3),
+    "gray4k": dict(W=3840, H=2160, C=1, N=200000, P=1, wl=[515e-9], pitch=3.74e-6, d_val=1e-3, vd=0.0),
+}
+
+
+def _field(C, H, W, seed=0):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    a = torch.rand((C, H, W), device="cuda", generator=g) * 1.2
+    ph = torch.rand((C, H, W), device="cuda", generator=g) * 6.283
+    return torch.polar(a, ph).contiguous()
+
+
+def run(stage, workload, iters=3, warmup=1):
+    w = WORKLOADS[workload]
+    C, H, W, P = w["C"], w["H"], w["W"], w["P"]
+    pad = reference_pad_size((W, H))
+    dist = reference_distances(P, w["vd"], w["d_val"])
+    times = []
+    if stage in ("blasm_fwd", "blasm_adj"):
+        plan = BlasmPlan(C, H, W, pad, w["wl"], dist, w["pitch"], aperture_radius=10 * max(W, H))
+        f = _field(C, H, W)
+        out = plan.forward(f)
+        g = _field(P * C, H, W, seed=1).view(P, C, H, W) if stage == "blasm_adj" else None
+        gin = torch.empty_like(f)
+        for i in range(warmup + iters):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            if stage == "blasm_fwd":
+                plan.forward(f, out=out)
+            else:
+                plan.backward(f, g, out=gin)
+            e.record()
+            torch.cuda.synchronize()
+            if i >= warmup:
+                times.append(s.elapsed_time(e))
+    elif stage == "render":
+        from .rasterizer import render_forward
+        rng = np.random.default_rng(0)
+        N = w["N"]
+        means = torch.from_numpy(np.stack([rng.uniform(0, W, N), rng.uniform(0, H, N)], 1).astype(np.float32)).cuda()
+        inv = torch.tensor([0.22, 0.01, 0.2], device="cuda").repeat(N, 1)
+        col = torch.rand(N, C, device="cuda")
+        ph = torch.rand(N, C, device="cuda") * 6.28
+        z = torch.rand(N, device="cuda")
+        radii = torch.full((N,), 12, dtype=torch.int32, device="cuda")
+        k = (2 * np.pi / torch.tensor(w["wl"], dtype=torch.float32)).cuda()
+        for i in range(warmup + iters):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            render_forward(means, inv, col, ph, z, z * 500, z + 4, k, w["pitch"] ** 2, W, H, radii=radii)
+            e.record()
+            torch.cuda.synchronize()
+            if i >= warmup:
+                times.append(s.elapsed_time(e))
+    else:
+        raise ValueError(stage)
+    return {"stage": stage, "workload": workload, "ms": float(np.mean(times)), "iters": iters}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--stage", default="blasm_fwd", choices=["blasm_fwd", "blasm_adj", "render"])
+    ap.add_argument("--workload", default="rgb1080", choices=sorted(WORKLOADS))
+    ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
+    a = ap.parse_args()
+    print(json.dumps(run(a.stage, a.workload, a.iters, a.warmup)))
+
+
+if __name__ == "__main__":
+    main()
