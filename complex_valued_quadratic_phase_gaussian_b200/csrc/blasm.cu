@@ -21,7 +21,7 @@
 #include <cstring>
 #include <vector>
 
-#include "blasm.cuh"
+#include "blasm_cols.cuh"
 
 namespace cvqpg {
 
@@ -55,57 +55,14 @@ bool make_fft_plan(int n, FftPlan* plan) {
 }
 
 // ---------------------------------------------------------------------------
-// device helpers
+// forward kernels. Intermediates are row-major: A [C][pH][NW] after the row
+// pass, B [P*C][out_h][NW] after the column pass. The column pass reads and
+// writes one column per CTA at a stride of NW; neighbouring columns are
+// handled by neighbouring CTAs at the same time, so the 32-byte sectors are
+// completed in L2.
 // ---------------------------------------------------------------------------
-// Transfer function times 1/(NH*NW) at natural FFT index (ky, kx).
-__device__ __forceinline__ float2 transfer(const BlasmDev& d, const PCParam& pp, int c, int ky, int kx) {
-    int j = ky + (d.NH >> 1);
-    if (j >= d.NH) j -= d.NH;
-    int i = kx + (d.NW >> 1);
-    if (i >= d.NW) i -= d.NW;
-    if (j < pp.j0 || j >= pp.j1) return make_float2(0.f, 0.f);
-    const int2 ap = d.aperture[j];
-    const int lo = max(pp.i0, ap.x), hi = min(pp.i1, ap.y);
-    if (i < lo || i >= hi) return make_float2(0.f, 0.f);
-    const float u = __ldg(&d.a_row[c * d.NH + j]) + __ldg(&d.b_col[c * d.NW + i]);
-    if (!(u < 1.0f)) return make_float2(0.f, 0.f);  // evanescent: excluded
-    // 2 pi z sqrt(1/lambda^2 - f^2) = theta0 + K (sqrt(1-u) - 1),  sqrt(1-u) - 1 = -u / (1 + sqrt(1-u))
-    const float th = pp.theta0 - pp.K * u / (1.0f + sqrtf(1.0f - u));
-    float sn, cs;
-    sincos_reduced(th, &sn, &cs);
-    return make_float2(cs * d.scale, sn * d.scale);
-}
-
-// amplitude clamp to 1 keeping the phase (reference: generate_complex_field(clamp(|U|,0,1), angle(U)))
-__device__ __forceinline__ float2 clamp_amplitude(float2 u) {
-    const float r2 = u.x * u.x + u.y * u.y;
-    if (r2 <= 1.0f) return u;
-    const float inv = rsqrtf(r2);
-    return make_float2(u.x * inv, u.y * inv);
-}
-
-// adjoint of clamp_amplitude at u for the incoming gradient g (torch convention)
-__device__ __forceinline__ float2 clamp_amplitude_adjoint(float2 u, float2 g) {
-    const float r2 = u.x * u.x + u.y * u.y;
-    if (r2 == 0.0f) return make_float2(0.f, 0.f);
-    if (r2 <= 1.0f) return g;
-    const float r = sqrtf(r2);
-    const float c = u.x / r, s = u.y / r;
-    const float gphi = -g.x * s + g.y * c;
-    return make_float2(-gphi * u.y / r2, gphi * u.x / r2);
-}
-
-// ---------------------------------------------------------------------------
-// forward kernels
-// ---------------------------------------------------------------------------
-constexpr int kRowThreads = 256;
-constexpr int kColThreads = 512;
-
-__host__ __device__ constexpr int ilog2c(int g) { return g >= 4 ? 2 : (g >= 2 ? 1 : 0); }
-
 // K1: one padded row per CTA. The first FFT pass reads the splat field directly
-// (replicate guard band, Tukey window, amplitude clamp on the fly); output in
-// the tiled layout [C][NW/G][pH][G] that the column pass reads contiguously.
+// (replicate guard band, Tukey window, amplitude clamp on the fly).
 __global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_kernel(BlasmDev d, const float2* __restrict__ in,
                                                                      float2* __restrict__ A) {
     extern __shared__ float2 sm[];
@@ -141,56 +98,42 @@ __global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_kernel(BlasmDev d,
             },
             b0, b1, ld, 0, d.row, false);
     }
-    const int G = d.G, ngroups = d.NW / G;
-    for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) {
-        const int gi = kx / G, g = kx - gi * G;
-        A[(((size_t)c * ngroups + gi) * d.pH + y) * G + g] = res[fft_pad(kx)];
-    }
+    float2* dst = A + ((size_t)c * d.pH + y) * d.NW;
+    for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) dst[kx] = res[fft_pad(kx)];
 }
 
-// K2: G columns per CTA: forward FFT (length NH) once, then per plane an
-// inverse FFT whose first pass multiplies by the transfer function on load;
-// keep out_h rows -> B [P*C][out_h][NW].
-template <int G>
-__global__ void __launch_bounds__(kColThreads, 1) blasm_cols_fwd_kernel(BlasmDev d, const float2* __restrict__ A,
-                                                                        float2* __restrict__ B) {
+// K2 (generic variant, any plan): the spectrum stays in a third shared buffer.
+__global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_kernel(BlasmDev d, const float2* __restrict__ A,
+                                                                     float2* __restrict__ B) {
     extern __shared__ float2 sm[];
-    constexpr int TS = ilog2c(G);
-    const int ld = fft_ld(d.NH);
-    float2* buf[3] = {sm, sm + G * ld, sm + 2 * G * ld};
-    const int ngroups = d.NW / G;
-    const int c = blockIdx.x / ngroups, gi = blockIdx.x - c * ngroups;
-    const int kx0 = gi * G;
-    const int y0 = (d.NH >> 1) - (d.pH >> 1);
-    const int pH = d.pH;
-    const float2* src = A + ((size_t)c * ngroups + gi) * pH * G;
+    const int NH = d.NH, NW = d.NW, ld = fft_ld(NH);
+    float2* buf[3] = {sm, sm + ld, sm + 2 * ld};
+    const int c = blockIdx.x / NW, kx = blockIdx.x - c * NW;
+    const int y0 = (NH >> 1) - (d.pH >> 1), pH = d.pH;
+    const float2* src = A + (size_t)c * pH * NW + kx;
     float2* spec = fft_run(
-        [=](int t, int e) {
+        [=](int, int e) {
             const int y = e - y0;
-            return (y < 0 || y >= pH) ? make_float2(0.f, 0.f) : __ldg(&src[y * G + t]);
+            return (y < 0 || y >= pH) ? make_float2(0.f, 0.f) : __ldg(&src[(size_t)y * NW]);
         },
-        buf[0], buf[1], ld, TS, d.col, false);
+        buf[0], buf[1], ld, 0, d.col, false);
     float2* w0 = spec == buf[0] ? buf[1] : buf[0];
     float2* w1 = buf[2];
-    const int row0 = (d.NH >> 1) - (d.out_h >> 1);
+    const int row0 = (NH >> 1) - (d.out_h >> 1);
     for (int p = 0; p < d.P; p++) {
         const int pc = p * d.C + c;
         const PCParam pp = d.pcp[pc];
         const float2* sp = spec;
-        float2* res = fft_run(
-            [=](int t, int e) { return cmul(sp[t * ld + fft_pad(e)], transfer(d, pp, c, e, kx0 + t)); }, w0, w1, ld,
-            TS, d.col, true);
-        float2* dst = B + (size_t)pc * d.out_h * d.NW + kx0;
-        for (int e = threadIdx.x; e < d.out_h * G; e += blockDim.x) {
-            const int y = e >> TS, g = e & (G - 1);
-            dst[(size_t)y * d.NW + g] = res[g * ld + fft_pad(row0 + y)];
-        }
+        float2* res = fft_run([=](int, int e) { return cmul(sp[fft_pad(e)], transfer(d, pp, c, e, kx)); }, w0, w1, ld,
+                              0, d.col, true);
+        float2* dst = B + (size_t)pc * d.out_h * NW + kx;
+        for (int y = threadIdx.x; y < d.out_h; y += blockDim.x) dst[(size_t)y * NW] = res[fft_pad(row0 + y)];
         __syncthreads();
     }
 }
 
 // K3: inverse FFT of a kept row (first pass reads global), keep out_w columns
-// -> V [P*C][out_h][out_w]
+// -> V [P*C][out_h][out_w] and optionally pred = clamp(|V|^2, 0, 1)
 __global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_kernel(BlasmDev d, const float2* __restrict__ B,
                                                                      float2* __restrict__ V,
                                                                      float* __restrict__ pred) {
@@ -215,10 +158,9 @@ __global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_kernel(BlasmDev d,
 }
 
 // ---------------------------------------------------------------------------
-// adjoint kernels
+// adjoint kernels (same layouts: Bt [P*C][out_h][NW], Ab [C][in_h][NW])
 // ---------------------------------------------------------------------------
-// K3b: gradient row embedded at the out_w centred columns -> forward FFT ->
-// tiled [P*C][NW/G][out_h][G]
+// K3b: gradient row embedded at the out_w centred columns -> forward FFT
 __global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_adj_kernel(BlasmDev d, const float2* __restrict__ gV,
                                                                          const float* __restrict__ gpred,
                                                                          const float2* __restrict__ Vf,
@@ -226,7 +168,6 @@ __global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_adj_kernel(BlasmDe
     extern __shared__ float2 sm[];
     const int ld = fft_ld(d.NW);
     const int row = blockIdx.x;
-    const int pc = row / d.out_h, y = row - pc * d.out_h;
     const int col0 = (d.NW >> 1) - (d.out_w >> 1);
     const int ow = d.out_w;
     float2* res;
@@ -252,71 +193,51 @@ __global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_adj_kernel(BlasmDe
             },
             sm, sm + ld, ld, 0, d.row, false);
     }
-    const int G = d.G, ngroups = d.NW / G;
-    for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) {
-        const int gi = kx / G, g = kx - gi * G;
-        Bt[(((size_t)pc * ngroups + gi) * d.out_h + y) * G + g] = res[fft_pad(kx)];
-    }
+    float2* dst = Bt + (size_t)row * d.NW;
+    for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) dst[kx] = res[fft_pad(kx)];
 }
 
-// K2b: per plane forward column FFT (first pass reads the tiled gradient rows),
-// multiply by conj(transfer) and accumulate in registers; then one inverse FFT
-// of the sum; keep the input rows -> Ab [C][in_h][NW]
-template <int G, int E>
-__global__ void __launch_bounds__(kColThreads, 1) blasm_cols_adj_kernel(BlasmDev d, const float2* __restrict__ Bt,
-                                                                        float2* __restrict__ Ab) {
+// K2b (generic variant): accumulator in registers over a fixed element mapping.
+template <int E>
+__global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_kernel(BlasmDev d, const float2* __restrict__ Bt,
+                                                                     float2* __restrict__ Ab) {
     extern __shared__ float2 sm[];
-    constexpr int TS = ilog2c(G);
-    const int ld = fft_ld(d.NH);
+    const int NH = d.NH, NW = d.NW, ld = fft_ld(NH);
     float2* b0 = sm;
-    float2* b1 = sm + G * ld;
-    const int ngroups = d.NW / G;
-    const int c = blockIdx.x / ngroups, gi = blockIdx.x - c * ngroups;
-    const int kx0 = gi * G;
-    const int row0 = (d.NH >> 1) - (d.out_h >> 1);
-    const int oh = d.out_h;
-    const int total = G * d.NH;
+    float2* b1 = sm + ld;
+    const int c = blockIdx.x / NW, kx = blockIdx.x - c * NW;
+    const int row0 = (NH >> 1) - (d.out_h >> 1), oh = d.out_h;
     float2 acc[E];
 #pragma unroll
     for (int i = 0; i < E; i++) acc[i] = make_float2(0.f, 0.f);
     for (int p = 0; p < d.P; p++) {
         const int pc = p * d.C + c;
-        const float2* src = Bt + ((size_t)pc * ngroups + gi) * oh * G;
+        const float2* src = Bt + (size_t)pc * oh * NW + kx;
         float2* res = fft_run(
-            [=](int t, int e) {
+            [=](int, int e) {
                 const int y = e - row0;
-                return (y < 0 || y >= oh) ? make_float2(0.f, 0.f) : __ldg(&src[y * G + t]);
+                return (y < 0 || y >= oh) ? make_float2(0.f, 0.f) : __ldg(&src[(size_t)y * NW]);
             },
-            b0, b1, ld, TS, d.col, false);
+            b0, b1, ld, 0, d.col, false);
         const PCParam pp = d.pcp[pc];
 #pragma unroll
         for (int i = 0; i < E; i++) {
-            const int e = threadIdx.x + i * blockDim.x;
-            if (e < total) {
-                const int t = e & (G - 1), ky = e >> TS;
-                acc[i] = cadd(acc[i], cmulc(res[t * ld + fft_pad(ky)], transfer(d, pp, c, ky, kx0 + t)));
-            }
+            const int ky = threadIdx.x + i * blockDim.x;
+            if (ky < NH) acc[i] = cadd(acc[i], cmulc(res[fft_pad(ky)], transfer(d, pp, c, ky, kx)));
         }
         __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < E; i++) {
-        const int e = threadIdx.x + i * blockDim.x;
-        if (e < total) {
-            const int t = e & (G - 1), ky = e >> TS;
-            b0[t * ld + fft_pad(ky)] = acc[i];
-        }
+        const int ky = threadIdx.x + i * blockDim.x;
+        if (ky < NH) b0[fft_pad(ky)] = acc[i];
     }
     __syncthreads();
-    const float2* s0 = b0;
-    float2* res = fft_run([=](int t, int e) { return s0[t * ld + fft_pad(e)]; }, b1, b0, ld, TS, d.col, true);
+    float2* res = fft_run([b0](int, int e) { return b0[fft_pad(e)]; }, b1, b0, ld, 0, d.col, true);
     const int in_h = d.input_mode == 0 ? d.H : d.pH;
-    const int r0 = (d.NH >> 1) - (in_h >> 1);
-    float2* dst = Ab + (size_t)c * in_h * d.NW + kx0;
-    for (int e = threadIdx.x; e < in_h * G; e += blockDim.x) {
-        const int y = e >> TS, g = e & (G - 1);
-        dst[(size_t)y * d.NW + g] = res[g * ld + fft_pad(r0 + y)];
-    }
+    const int r0 = (NH >> 1) - (in_h >> 1);
+    float2* dst = Ab + (size_t)c * in_h * NW + kx;
+    for (int y = threadIdx.x; y < in_h; y += blockDim.x) dst[(size_t)y * NW] = res[fft_pad(r0 + y)];
 }
 
 // K1b: inverse row FFT (first pass reads global), keep the input columns,
@@ -435,11 +356,9 @@ int blasm_make_dev(const cvqpg_blasm_params* p, const void* tables, size_t table
     d->out_h = p->out_height > 0 ? p->out_height : d->H;
     d->out_w = p->out_width > 0 ? p->out_width : d->W;
     d->input_mode = p->input_mode;
-    // columns per column-pass CTA: the widest of 2, 1 whose three ping-pong
-    // buffers fit in shared memory
-    d->G = (size_t)3 * 2 * fft_ld(d->NH) * sizeof(float2) <= 227 * 1024 ? 2 : 1;
-    if ((size_t)3 * d->G * fft_ld(d->NH) * sizeof(float2) > 227 * 1024) return CVQPG_ERR_UNSUPPORTED;
-    if (d->NW % d->G) return CVQPG_ERR_UNSUPPORTED;
+    // one column per column-pass CTA (row-major intermediates)
+    d->G = 1;
+    if ((size_t)3 * fft_ld(d->NH) * sizeof(float2) > 227 * 1024) return CVQPG_ERR_UNSUPPORTED;
     d->scale = (float)(1.0 / ((double)d->NH * (double)d->NW));
     make_fft_plan(d->NW, &d->row);
     make_fft_plan(d->NH, &d->col);
@@ -468,32 +387,80 @@ static void carve(const BlasmDev& d, void* ws, float2** A, float2** B) {
 }
 
 static size_t row_smem(const BlasmDev& d) { return (size_t)2 * fft_ld(d.NW) * sizeof(float2); }
-static size_t col_fwd_smem(const BlasmDev& d) { return (size_t)3 * d.G * fft_ld(d.NH) * sizeof(float2); }
-static size_t col_adj_smem(const BlasmDev& d) { return (size_t)2 * d.G * fft_ld(d.NH) * sizeof(float2); }
+static size_t col2_smem(const BlasmDev& d) { return (size_t)2 * fft_ld(d.NH) * sizeof(float2); }
+static size_t col3_smem(const BlasmDev& d) { return (size_t)3 * fft_ld(d.NH) * sizeof(float2); }
 constexpr size_t kSmemMax = 227 * 1024;
 
 #define CVQPG_SMEM_ATTR(kern, bytes) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(bytes))
 
-template <int G>
-static void launch_cols_fwd(const BlasmDev& d, const float2* A, float2* B, cudaStream_t s) {
-    const size_t sm = col_fwd_smem(d);
-    CVQPG_SMEM_ATTR(blasm_cols_fwd_kernel<G>, sm);
-    blasm_cols_fwd_kernel<G><<<d.C * (d.NW / G), kColThreads, sm, s>>>(d, A, B);
+// Pick the radix whose butterflies stay in registers between the column FFTs:
+// the supported radix of the plan with the smallest register footprint
+// (butterflies per thread x radix). Returns false when no variant applies.
+static bool column_split(const FftPlan& plan, ColSplit* cs) {
+    static const int kRL[] = {3, 5, 7, 8, 11, 13, 16};
+    int best = -1, best_mb = 0, best_score = 1 << 30;
+    for (int p = 0; p < plan.npass; p++) {
+        const int r = (int)((plan.code >> (5 * p)) & 31ull);
+        bool ok = false;
+        for (int q : kRL) ok |= (q == r);
+        if (!ok || plan.npass < 2) continue;
+        const int nb = plan.n / r;
+        const int mb = (nb + kColThreads - 1) / kColThreads;
+        const int mbr = mb <= 1 ? 1 : (mb <= 2 ? 2 : 0);
+        if (!mbr) continue;
+        const int score = mbr * r;
+        if (score < best_score) {
+            best_score = score;
+            best = p;
+            best_mb = mbr;
+        }
+    }
+    if (best < 0) return false;
+    cs->rl = (int)((plan.code >> (5 * best)) & 31ull);
+    cs->mb = best_mb;
+    cs->head_code = 0;
+    cs->head_npass = 0;
+    for (int p = 0; p < plan.npass; p++) {
+        if (p == best) continue;
+        const unsigned long long r = (plan.code >> (5 * p)) & 31ull;
+        cs->head_code |= r << (5 * cs->head_npass);
+        cs->head_npass++;
+    }
+    return true;
 }
 
-template <int G, int E>
-static void launch_cols_adj(const BlasmDev& d, const float2* Bt, float2* Ab, cudaStream_t s) {
-    const size_t sm = col_adj_smem(d);
-    CVQPG_SMEM_ATTR((blasm_cols_adj_kernel<G, E>), sm);
-    blasm_cols_adj_kernel<G, E><<<d.C * (d.NW / G), kColThreads, sm, s>>>(d, Bt, Ab);
-}
-
-template <int G>
-static void dispatch_cols_adj(const BlasmDev& d, const float2* Bt, float2* Ab, cudaStream_t s) {
-    const int e = (G * d.NH + kColThreads - 1) / kColThreads;
-    if (e <= 8) launch_cols_adj<G, 8>(d, Bt, Ab, s);
-    else if (e <= 16) launch_cols_adj<G, 16>(d, Bt, Ab, s);
-    else launch_cols_adj<G, 32>(d, Bt, Ab, s);
+static void launch_columns(bool adjoint, const BlasmDev& d, const float2* in, float2* out, cudaStream_t s) {
+    ColSplit cs;
+    if (column_split(d.col, &cs)) {
+        switch (cs.rl) {
+            case 3: launch_cols_reg_r3(adjoint, d, cs, in, out, s); return;
+            case 5: launch_cols_reg_r5(adjoint, d, cs, in, out, s); return;
+            case 7: launch_cols_reg_r7(adjoint, d, cs, in, out, s); return;
+            case 8: launch_cols_reg_r8(adjoint, d, cs, in, out, s); return;
+            case 11: launch_cols_reg_r11(adjoint, d, cs, in, out, s); return;
+            case 13: launch_cols_reg_r13(adjoint, d, cs, in, out, s); return;
+            case 16: launch_cols_reg_r16(adjoint, d, cs, in, out, s); return;
+            default: break;
+        }
+    }
+    if (!adjoint) {
+        const size_t sm = col3_smem(d);
+        CVQPG_SMEM_ATTR(blasm_cols_fwd_kernel, sm);
+        blasm_cols_fwd_kernel<<<d.C * d.NW, kColThreads, sm, s>>>(d, in, out);
+    } else {
+        const size_t sm = col2_smem(d);
+        const int e = (d.NH + kColThreads - 1) / kColThreads;
+        if (e <= 8) {
+            CVQPG_SMEM_ATTR(blasm_cols_adj_kernel<8>, sm);
+            blasm_cols_adj_kernel<8><<<d.C * d.NW, kColThreads, sm, s>>>(d, in, out);
+        } else if (e <= 16) {
+            CVQPG_SMEM_ATTR(blasm_cols_adj_kernel<16>, sm);
+            blasm_cols_adj_kernel<16><<<d.C * d.NW, kColThreads, sm, s>>>(d, in, out);
+        } else {
+            CVQPG_SMEM_ATTR(blasm_cols_adj_kernel<32>, sm);
+            blasm_cols_adj_kernel<32><<<d.C * d.NW, kColThreads, sm, s>>>(d, in, out);
+        }
+    }
 }
 
 void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace, cudaStream_t s,
@@ -504,9 +471,7 @@ void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred
     CVQPG_SMEM_ATTR(blasm_rows_fwd_kernel, rs);
     blasm_rows_fwd_kernel<<<d.C * d.pH, kRowThreads, rs, s>>>(d, in, A);
     if (marks) marks->mark(s);
-    if (d.G == 4) launch_cols_fwd<4>(d, A, B, s);
-    else if (d.G == 2) launch_cols_fwd<2>(d, A, B, s);
-    else launch_cols_fwd<1>(d, A, B, s);
+    launch_columns(false, d, A, B, s);
     if (marks) marks->mark(s);
     CVQPG_SMEM_ATTR(blasm_rows_inv_kernel, rs);
     blasm_rows_inv_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, B, out, pred);
@@ -521,9 +486,7 @@ void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* gra
     CVQPG_SMEM_ATTR(blasm_rows_fwd_adj_kernel, rs);
     blasm_rows_fwd_adj_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, grad_out, grad_pred, vfield, B);
     if (marks) marks->mark(s);
-    if (d.G == 4) dispatch_cols_adj<4>(d, B, A, s);
-    else if (d.G == 2) dispatch_cols_adj<2>(d, B, A, s);
-    else dispatch_cols_adj<1>(d, B, A, s);
+    launch_columns(true, d, B, A, s);
     if (marks) marks->mark(s);
     const int in_h = d.input_mode == 0 ? d.H : d.pH;
     CVQPG_SMEM_ATTR(blasm_rows_inv_adj_kernel, rs);
@@ -532,8 +495,7 @@ void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* gra
 }
 
 static bool fits(const BlasmDev& d) {
-    return row_smem(d) <= kSmemMax && col_fwd_smem(d) <= kSmemMax &&
-           (d.G * d.NH + kColThreads - 1) / kColThreads <= 32;
+    return row_smem(d) <= kSmemMax && col3_smem(d) <= kSmemMax && (d.NH + kColThreads - 1) / kColThreads <= 32;
 }
 
 }  // namespace cvqpg

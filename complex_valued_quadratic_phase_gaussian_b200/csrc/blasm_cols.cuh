@@ -1,0 +1,266 @@
+// Device helpers and the register-spectrum column kernels of the BLASM passes,
+// shared by blasm.cu and the per-radix instantiation units blasm_cols_r*.cu.
+#pragma once
+
+#include "blasm.cuh"
+
+namespace cvqpg {
+
+constexpr int kRowThreads = 256;
+constexpr int kColThreads = 256;
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+// Phase of the band-limited transfer function relative to theta0:
+//   2 pi z sqrt(1/lambda^2 - f^2) = theta0 - K u / (1 + sqrt(1 - u)),   u = lambda^2 f^2,
+// with u / (1 + sqrt(1-u)) = u/2 + u^2/8 + u^3/16 + 5u^4/128 + 7u^5/256 + O(u^6) for small u
+// (truncation below 3e-8 rad for u < 0.02 at K = 2e4).
+__device__ __forceinline__ float blasm_excess(float u) {
+    if (u < 0.02f) return u * fmaf(u, fmaf(u, fmaf(u, fmaf(u, 0.02734375f, 0.0390625f), 0.0625f), 0.125f), 0.5f);
+    return u / (1.0f + sqrtf(1.0f - u));
+}
+
+// Transfer function times 1/(NH*NW) at centred indices (j, i), column terms hoisted.
+__device__ __forceinline__ float2 transfer_ji(const BlasmDev& d, const PCParam& pp, int c, int j, int i, float bcol) {
+    if (j < pp.j0 || j >= pp.j1) return make_float2(0.f, 0.f);
+    const int2 ap = d.aperture[j];
+    if (i < ap.x || i >= ap.y) return make_float2(0.f, 0.f);
+    const float u = __ldg(&d.a_row[c * d.NH + j]) + bcol;
+    if (!(u < 1.0f)) return make_float2(0.f, 0.f);  // evanescent: excluded
+    float sn, cs;
+    sincos_reduced(pp.theta0 - pp.K * blasm_excess(u), &sn, &cs);
+    return make_float2(cs * d.scale, sn * d.scale);
+}
+
+// ... at natural FFT index (ky, kx)
+__device__ __forceinline__ float2 transfer(const BlasmDev& d, const PCParam& pp, int c, int ky, int kx) {
+    int j = ky + (d.NH >> 1);
+    if (j >= d.NH) j -= d.NH;
+    int i = kx + (d.NW >> 1);
+    if (i >= d.NW) i -= d.NW;
+    if (i < pp.i0 || i >= pp.i1) return make_float2(0.f, 0.f);
+    return transfer_ji(d, pp, c, j, i, __ldg(&d.b_col[c * d.NW + i]));
+}
+
+// amplitude clamp to 1 keeping the phase (reference: generate_complex_field(clamp(|U|,0,1), angle(U)))
+__device__ __forceinline__ float2 clamp_amplitude(float2 u) {
+    const float r2 = u.x * u.x + u.y * u.y;
+    if (r2 <= 1.0f) return u;
+    const float inv = rsqrtf(r2);
+    return make_float2(u.x * inv, u.y * inv);
+}
+
+// adjoint of clamp_amplitude at u for the incoming gradient g (torch convention)
+__device__ __forceinline__ float2 clamp_amplitude_adjoint(float2 u, float2 g) {
+    const float r2 = u.x * u.x + u.y * u.y;
+    if (r2 == 0.0f) return make_float2(0.f, 0.f);
+    if (r2 <= 1.0f) return g;
+    const float r = sqrtf(r2);
+    const float c = u.x / r, s = u.y / r;
+    const float gphi = -g.x * s + g.y * c;
+    return make_float2(-gphi * u.y / r2, gphi * u.x / r2);
+}
+
+// Column plan split for the register-held spectrum: the last forward radix RL
+// (compile time) and the remaining passes (`head`), used both after the first
+// inverse pass and before the last forward pass.
+struct ColSplit {
+    unsigned long long head_code;
+    int head_npass;
+    int rl;
+    int mb;
+};
+
+// K2 (register-spectrum variant): one column per CTA. Forward column FFT;
+// the last forward pass leaves its butterflies in registers; for each plane the
+// first inverse pass (same radix, same elements) multiplies by the transfer
+// function straight from registers. Two shared buffers per column.
+template <int RL, int MB>
+__global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(BlasmDev d, ColSplit cs,
+                                                                         const float2* __restrict__ A,
+                                                                         float2* __restrict__ B) {
+    extern __shared__ float2 sm[];
+    const int NH = d.NH, NW = d.NW, ld = fft_ld(NH);
+    float2* b0 = sm;
+    float2* b1 = sm + ld;
+    const int c = blockIdx.x / NW, kx = blockIdx.x - c * NW;
+    const int y0 = (NH >> 1) - (d.pH >> 1), pH = d.pH;
+    const float2* src = A + (size_t)c * pH * NW + kx;
+    const float2* tw = d.col.tw;
+    float2* buf = fft_run_passes(
+        [=](int, int e) {
+            const int y = e - y0;
+            return (y < 0 || y >= pH) ? make_float2(0.f, 0.f) : __ldg(&src[(size_t)y * NW]);
+        },
+        b0, b1, ld, 0, NH, cs.head_code, cs.head_npass, 1, tw, false);
+    const int nbL = NH / RL;  // = stride Ns of the last pass; k = j, twiddle stride 1
+    float2 spec[MB][RL];
+#pragma unroll
+    for (int b = 0; b < MB; b++) {
+        const int j = threadIdx.x + b * blockDim.x;
+        if (j < nbL) {
+            float2 v[RL];
+#pragma unroll
+            for (int r = 0; r < RL; r++) v[r] = buf[fft_pad(j + r * nbL)];
+            apply_twiddles<RL>(v, __ldg(&tw[j]));
+            dft<RL>(v, false);
+#pragma unroll
+            for (int r = 0; r < RL; r++) spec[b][r] = v[r];
+        }
+    }
+    __syncthreads();
+    int i = kx + (NW >> 1);
+    if (i >= NW) i -= NW;
+    const int row0 = (NH >> 1) - (d.out_h >> 1);
+    for (int p = 0; p < d.P; p++) {
+        const int pc = p * d.C + c;
+        const PCParam pp = d.pcp[pc];
+        const bool col_ok = i >= pp.i0 && i < pp.i1;
+        const float bcol = __ldg(&d.b_col[c * NW + i]);
+#pragma unroll
+        for (int b = 0; b < MB; b++) {
+            const int j = threadIdx.x + b * blockDim.x;
+            if (j < nbL) {
+                float2 v[RL];
+#pragma unroll
+                for (int r = 0; r < RL; r++) {
+                    int jj = j + r * nbL + (NH >> 1);
+                    if (jj >= NH) jj -= NH;
+                    v[r] = col_ok ? cmul(spec[b][r], transfer_ji(d, pp, c, jj, i, bcol)) : make_float2(0.f, 0.f);
+                }
+                dft<RL>(v, true);
+#pragma unroll
+                for (int r = 0; r < RL; r++) b0[fft_pad(j * RL + r)] = v[r];
+            }
+        }
+        __syncthreads();
+        float2* res = fft_run_passes([b0](int, int e) { return b0[fft_pad(e)]; }, b1, b0, ld, 0, NH, cs.head_code,
+                                     cs.head_npass, RL, tw, true);
+        float2* dst = B + (size_t)pc * d.out_h * NW + kx;
+        for (int y = threadIdx.x; y < d.out_h; y += blockDim.x) dst[(size_t)y * NW] = res[fft_pad(row0 + y)];
+        __syncthreads();
+    }
+}
+
+// K2b (register variant): per plane forward column FFT whose last pass leaves
+// its butterflies in registers, multiplied by conj(transfer) and accumulated
+// there; then the first inverse pass starts from the accumulator.
+template <int RL, int MB>
+__global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(BlasmDev d, ColSplit cs,
+                                                                         const float2* __restrict__ Bt,
+                                                                         float2* __restrict__ Ab) {
+    extern __shared__ float2 sm[];
+    const int NH = d.NH, NW = d.NW, ld = fft_ld(NH);
+    float2* b0 = sm;
+    float2* b1 = sm + ld;
+    const int c = blockIdx.x / NW, kx = blockIdx.x - c * NW;
+    const int row0 = (NH >> 1) - (d.out_h >> 1), oh = d.out_h;
+    const float2* tw = d.col.tw;
+    const int nbL = NH / RL;
+    int i = kx + (NW >> 1);
+    if (i >= NW) i -= NW;
+    const float bcol = __ldg(&d.b_col[c * NW + i]);
+    float2 acc[MB][RL];
+#pragma unroll
+    for (int b = 0; b < MB; b++)
+#pragma unroll
+        for (int r = 0; r < RL; r++) acc[b][r] = make_float2(0.f, 0.f);
+    for (int p = 0; p < d.P; p++) {
+        const int pc = p * d.C + c;
+        const float2* src = Bt + (size_t)pc * oh * NW + kx;
+        float2* buf = fft_run_passes(
+            [=](int, int e) {
+                const int y = e - row0;
+                return (y < 0 || y >= oh) ? make_float2(0.f, 0.f) : __ldg(&src[(size_t)y * NW]);
+            },
+            b0, b1, ld, 0, NH, cs.head_code, cs.head_npass, 1, tw, false);
+        const PCParam pp = d.pcp[pc];
+        const bool col_ok = i >= pp.i0 && i < pp.i1;
+#pragma unroll
+        for (int b = 0; b < MB; b++) {
+            const int j = threadIdx.x + b * blockDim.x;
+            if (j < nbL) {
+                float2 v[RL];
+#pragma unroll
+                for (int r = 0; r < RL; r++) v[r] = buf[fft_pad(j + r * nbL)];
+                apply_twiddles<RL>(v, __ldg(&tw[j]));
+                dft<RL>(v, false);
+                if (col_ok) {
+#pragma unroll
+                    for (int r = 0; r < RL; r++) {
+                        int jj = j + r * nbL + (NH >> 1);
+                        if (jj >= NH) jj -= NH;
+                        acc[b][r] = cadd(acc[b][r], cmulc(v[r], transfer_ji(d, pp, c, jj, i, bcol)));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int b = 0; b < MB; b++) {
+        const int j = threadIdx.x + b * blockDim.x;
+        if (j < nbL) {
+            float2 v[RL];
+#pragma unroll
+            for (int r = 0; r < RL; r++) v[r] = acc[b][r];
+            dft<RL>(v, true);
+#pragma unroll
+            for (int r = 0; r < RL; r++) b0[fft_pad(j * RL + r)] = v[r];
+        }
+    }
+    __syncthreads();
+    float2* res = fft_run_passes([b0](int, int e) { return b0[fft_pad(e)]; }, b1, b0, ld, 0, NH, cs.head_code,
+                                 cs.head_npass, RL, tw, true);
+    const int in_h = d.input_mode == 0 ? d.H : d.pH;
+    const int r0 = (NH >> 1) - (in_h >> 1);
+    float2* dst = Ab + (size_t)c * in_h * NW + kx;
+    for (int y = threadIdx.x; y < in_h; y += blockDim.x) dst[(size_t)y * NW] = res[fft_pad(r0 + y)];
+}
+
+
+void launch_cols_reg_r3(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                        cudaStream_t s);
+void launch_cols_reg_r5(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                        cudaStream_t s);
+void launch_cols_reg_r7(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                        cudaStream_t s);
+void launch_cols_reg_r8(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                        cudaStream_t s);
+void launch_cols_reg_r11(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                         cudaStream_t s);
+void launch_cols_reg_r13(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                         cudaStream_t s);
+void launch_cols_reg_r16(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                         cudaStream_t s);
+
+// Instantiate the forward and adjoint register-spectrum kernels for one radix.
+#define CVQPG_DEFINE_COLS_REG(RL)                                                                                  \
+    void launch_cols_reg_r##RL(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out, \
+                               cudaStream_t s) {                                                                   \
+        const size_t sm = (size_t)2 * fft_ld(d.NH) * sizeof(float2);                                              \
+        if (!adjoint) {                                                                                            \
+            if (cs.mb == 1) {                                                                                      \
+                cudaFuncSetAttribute(blasm_cols_fwd_reg_kernel<RL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)sm);                                                                     \
+                blasm_cols_fwd_reg_kernel<RL, 1><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);              \
+            } else {                                                                                               \
+                cudaFuncSetAttribute(blasm_cols_fwd_reg_kernel<RL, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)sm);                                                                     \
+                blasm_cols_fwd_reg_kernel<RL, 2><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);              \
+            }                                                                                                      \
+        } else {                                                                                                   \
+            if (cs.mb == 1) {                                                                                      \
+                cudaFuncSetAttribute(blasm_cols_adj_reg_kernel<RL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)sm);                                                                     \
+                blasm_cols_adj_reg_kernel<RL, 1><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);              \
+            } else {                                                                                               \
+                cudaFuncSetAttribute(blasm_cols_adj_reg_kernel<RL, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)sm);                                                                     \
+                blasm_cols_adj_reg_kernel<RL, 2><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);              \
+            }                                                                                                      \
+        }                                                                                                          \
+    }
+
+}  // namespace cvqpg

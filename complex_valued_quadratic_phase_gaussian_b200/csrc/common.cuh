@@ -7,7 +7,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
-#include "../../include/cvqpg.h"
+#include "cvqpg.h"
 
 namespace cvqpg {
 

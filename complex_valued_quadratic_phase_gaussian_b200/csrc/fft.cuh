@@ -58,61 +58,59 @@ __device__ __forceinline__ void dft(float2 (&v)[R], bool inv) {
     } else if constexpr (R == 4) {
         dft4(v[0], v[1], v[2], v[3], inv);
     } else if constexpr (R == 8) {
-        float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-        float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
-        dft4(e0, e1, e2, e3, inv);
-        dft4(o0, o1, o2, o3, inv);
-        float2 e[4] = {e0, e1, e2, e3}, o[4] = {o0, o1, o2, o3};
+        // radix-2 x 4, in place: evens and odds transformed where they sit
+        dft4(v[0], v[2], v[4], v[6], inv);
+        dft4(v[1], v[3], v[5], v[7], inv);
+        float2 x[8];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const float2 w = make_float2(DftTab<8>::c(k), inv ? DftTab<8>::s(k) : -DftTab<8>::s(k));
-            const float2 t = k == 0 ? o[0] : cmul(o[k], w);
-            v[k] = cadd(e[k], t);
-            v[k + 4] = csub(e[k], t);
+            const float2 t = k == 0 ? v[1] : cmul(v[2 * k + 1], w);
+            x[k] = cadd(v[2 * k], t);
+            x[k + 4] = csub(v[2 * k], t);
         }
-    } else if constexpr (R == 16) {
-        float2 y[4][4];
 #pragma unroll
-        for (int n2 = 0; n2 < 4; n2++) {
-            y[n2][0] = v[n2];
-            y[n2][1] = v[4 + n2];
-            y[n2][2] = v[8 + n2];
-            y[n2][3] = v[12 + n2];
-            dft4(y[n2][0], y[n2][1], y[n2][2], y[n2][3], inv);
+        for (int k = 0; k < 8; k++) v[k] = x[k];
+    } else if constexpr (R == 16) {
+        // 4 x 4 in place: column DFTs over n1, twiddle W16^(n2 k1), row DFTs over n2,
+        // then the 4x4 transpose is a compile-time renaming of registers.
+#pragma unroll
+        for (int n2 = 0; n2 < 4; n2++) dft4(v[n2], v[4 + n2], v[8 + n2], v[12 + n2], inv);
+#pragma unroll
+        for (int n2 = 1; n2 < 4; n2++)
 #pragma unroll
             for (int k1 = 1; k1 < 4; k1++) {
-                if (n2 == 0) continue;
                 const int q = (n2 * k1) & 15;
                 const float2 w = make_float2(DftTab<16>::c(q), inv ? DftTab<16>::s(q) : -DftTab<16>::s(q));
-                y[n2][k1] = cmul(y[n2][k1], w);
+                v[4 * k1 + n2] = cmul(v[4 * k1 + n2], w);
             }
-        }
 #pragma unroll
-        for (int k1 = 0; k1 < 4; k1++) {
-            float2 a = y[0][k1], b = y[1][k1], c = y[2][k1], d = y[3][k1];
-            dft4(a, b, c, d, inv);
-            v[k1] = a;
-            v[k1 + 4] = b;
-            v[k1 + 8] = c;
-            v[k1 + 12] = d;
-        }
+        for (int k1 = 0; k1 < 4; k1++) dft4(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3], inv);
+        float2 x[16];
+#pragma unroll
+        for (int k1 = 0; k1 < 4; k1++)
+#pragma unroll
+            for (int k2 = 0; k2 < 4; k2++) x[k1 + 4 * k2] = v[4 * k1 + k2];
+#pragma unroll
+        for (int k = 0; k < 16; k++) v[k] = x[k];
     } else {
-        // odd R: X_k = x0 + sum_m (x_m + x_{R-m}) cos(2 pi m k/R) -/+ i (x_m - x_{R-m}) sin(2 pi m k/R)
+        // odd R: X_k = x0 + sum_m (x_m + x_{R-m}) cos(2 pi m k/R) -/+ i (x_m - x_{R-m}) sin(2 pi m k/R);
+        // the inputs are folded into a[], b[] first, then the outputs overwrite v.
         static_assert(R % 2 == 1, "odd radix expected");
         constexpr int h = (R - 1) / 2;
         float2 a[h], b[h];
-        float2 sum = v[0];
+        const float2 x0 = v[0];
+        float2 sum = x0;
 #pragma unroll
         for (int m = 1; m <= h; m++) {
             a[m - 1] = cadd(v[m], v[R - m]);
             b[m - 1] = csub(v[m], v[R - m]);
             sum = cadd(sum, a[m - 1]);
         }
-        float2 out[R];
-        out[0] = sum;
+        v[0] = sum;
 #pragma unroll
         for (int k = 1; k <= h; k++) {
-            float2 A = v[0], B = make_float2(0.f, 0.f);
+            float2 A = x0, B = make_float2(0.f, 0.f);
 #pragma unroll
             for (int m = 1; m <= h; m++) {
                 const int q = (m * k) % R;
@@ -122,23 +120,42 @@ __device__ __forceinline__ void dft(float2 (&v)[R], bool inv) {
                 B.y = fmaf(b[m - 1].y, DftTab<R>::s(q), B.y);
             }
             if (!inv) {
-                out[k] = make_float2(A.x + B.y, A.y - B.x);
-                out[R - k] = make_float2(A.x - B.y, A.y + B.x);
+                v[k] = make_float2(A.x + B.y, A.y - B.x);
+                v[R - k] = make_float2(A.x - B.y, A.y + B.x);
             } else {
-                out[k] = make_float2(A.x - B.y, A.y + B.x);
-                out[R - k] = make_float2(A.x + B.y, A.y - B.x);
+                v[k] = make_float2(A.x - B.y, A.y + B.x);
+                v[R - k] = make_float2(A.x + B.y, A.y - B.x);
             }
         }
-#pragma unroll
-        for (int r = 0; r < R; r++) v[r] = out[r];
     }
 }
 
+// v[r] *= w^r for r = 1..R-1, the powers formed by a running product: one
+// table load per butterfly instead of R-1 scattered ones, two live complex
+// values. The product chain adds at most R-2 roundings (~1e-6 relative at R=17).
+template <int R>
+__device__ __forceinline__ void apply_twiddles(float2 (&v)[R], float2 w1) {
+    float2 w = w1;
+#pragma unroll
+    for (int r = 1; r < R; r++) {
+        v[r] = cmul(v[r], w);
+        if (r + 1 < R) w = cmul(w, w1);
+    }
+}
+
+// Decompose a butterfly index j of a pass with stride Ns: q = j / Ns, k = j % Ns.
+// floor((j + 1/2) / Ns) evaluated in float is exact for j < 2^22: the true value
+// is at least 1/(2 Ns) from an integer and the float error is below j 2^-23 / Ns.
+__device__ __forceinline__ void split_index(int j, int Ns, float inv_ns, int& q, int& k) {
+    q = __float2int_rz(fmaf((float)j, inv_ns, 0.5f * inv_ns));
+    k = j - q * Ns;
+}
+
 // ---------------------------------------------------------------------------
-// one out-of-place Stockham pass over `ntrans` sequences. `src(t, a)` returns
-// element a of sequence t (a plain shared-memory read for every pass but the
-// first, where it can fuse a pointwise multiply into the load). Each thread
-// holds a single butterfly at a time, so the register footprint is one radix.
+// one out-of-place Stockham pass over 2^tshift interleaved sequences. `src(t, a)`
+// returns element a of sequence t (a shared-memory read, or for the first pass a
+// global read with a pointwise operation fused into it). Each thread holds a
+// single butterfly at a time, so the register footprint is one radix.
 // ---------------------------------------------------------------------------
 template <int R, typename Src>
 __device__ __forceinline__ void fft_pass(Src src, float2* __restrict__ out, int ld, int tshift, int n, int Ns,
@@ -146,22 +163,22 @@ __device__ __forceinline__ void fft_pass(Src src, float2* __restrict__ out, int 
     const int nb = n / R;
     const int total = nb << tshift;
     const int stride = n / (Ns * R);
+    const float inv_ns = 1.0f / (float)Ns;
+    const int tmask = (1 << tshift) - 1;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int t = idx & ((1 << tshift) - 1), j = idx >> tshift;  // sequences interleaved across lanes
-        const int k = j % Ns;
+        const int t = idx & tmask, j = idx >> tshift;
+        int q, k;
+        split_index(j, Ns, inv_ns, q, k);
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = src(t, j + r * nb);
         if (Ns > 1) {
-#pragma unroll
-            for (int r = 1; r < R; r++) {
-                float2 w = __ldg(&tw[r * k * stride]);
-                if (inv) w.y = -w.y;
-                v[r] = cmul(v[r], w);
-            }
+            float2 w = __ldg(&tw[k * stride]);
+            if (inv) w.y = -w.y;
+            apply_twiddles<R>(v, w);
         }
         dft<R>(v, inv);
-        const int o = (j / Ns) * Ns * R + k;
+        const int o = q * Ns * R + k;
         float2* dst = out + t * ld;
 #pragma unroll
         for (int r = 0; r < R; r++) dst[fft_pad(o + r * Ns)] = v[r];
@@ -187,31 +204,38 @@ __device__ __forceinline__ void fft_pass_dispatch(int R, Src src, float2* out, i
     }
 }
 
-// Full transform of 2^tshift sequences with ping-pong buffers a, b. The first
-// pass reads through `first` and writes a; later passes alternate. Returns the
-// buffer holding the result (a or b). The caller must synchronise before
-// `first` reads anything written earlier; the function ends with a barrier.
+// Run `npass` passes (radices packed 5 bits each in `code`, first one in the low
+// bits) starting at stride Ns0, ping-ponging a, b; the first pass reads through
+// `first` and writes a. Returns the buffer holding the result. The caller must
+// synchronise before `first` reads shared data written earlier; ends with a barrier.
 template <typename First>
-__device__ __forceinline__ float2* fft_run(First first, float2* a, float2* b, int ld, int tshift, FftPlan plan,
-                                           bool inv) {
-    const int n = plan.n;
-    int Ns = 1;
-    int R = (int)(plan.code & 31ull);
-    fft_pass_dispatch(R, first, a, ld, tshift, n, Ns, plan.tw, inv);
+__device__ __forceinline__ float2* fft_run_passes(First first, float2* a, float2* b, int ld, int tshift, int n,
+                                                  unsigned long long code, int npass, int Ns0, const float2* tw,
+                                                  bool inv) {
+    int Ns = Ns0;
+    int R = (int)(code & 31ull);
+    fft_pass_dispatch(R, first, a, ld, tshift, n, Ns, tw, inv);
     Ns *= R;
     float2* cur = a;
     float2* nxt = b;
-    for (int p = 1; p < plan.npass; p++) {
-        R = (int)((plan.code >> (5 * p)) & 31ull);
+    for (int p = 1; p < npass; p++) {
+        R = (int)((code >> (5 * p)) & 31ull);
         const float2* in = cur;
-        fft_pass_dispatch(R, [in, ld](int t, int e) { return in[t * ld + fft_pad(e)]; }, nxt, ld, tshift, n, Ns,
-                          plan.tw, inv);
+        fft_pass_dispatch(R, [in, ld](int t, int e) { return in[t * ld + fft_pad(e)]; }, nxt, ld, tshift, n, Ns, tw,
+                          inv);
         Ns *= R;
         float2* tmp = cur;
         cur = nxt;
         nxt = tmp;
     }
     return cur;
+}
+
+// Full transform of 2^tshift sequences (all passes of the plan from stride 1).
+template <typename First>
+__device__ __forceinline__ float2* fft_run(First first, float2* a, float2* b, int ld, int tshift, FftPlan plan,
+                                           bool inv) {
+    return fft_run_passes(first, a, b, ld, tshift, plan.n, plan.code, plan.npass, 1, plan.tw, inv);
 }
 
 // Host: factor n into supported radices (16/8/4/2 first, then 3..17).
