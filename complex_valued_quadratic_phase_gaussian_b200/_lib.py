@@ -43,7 +43,7 @@ _SIGNATURES = {
     "cvqpg_blasm_forward": [_p, _p, _sz, _p, _p, _p, _sz, _p],
     "cvqpg_blasm_backward": [_p, _p, _sz, _p, _p, _p, _p, _sz, _p],
     "cvqpg_loss_workspace_size": [_p, _psz],
-    "cvqpg_loss_target_range": [_p, _i, _i, _i, _i, _p, _p],
+    "cvqpg_loss_target_range": [_p, _i, _i, _i, _i, _p, _p, _sz, _p],
     "cvqpg_loss_forward_backward": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
     "cvqpg_fit_workspace_size": [_p, _psz],
     "cvqpg_fit_setup": [_p, _p, _p, _sz],

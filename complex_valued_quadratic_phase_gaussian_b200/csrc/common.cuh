@@ -76,7 +76,7 @@ __device__ __forceinline__ void sincos_reduced(float x, float* s, float* c) {
 // ---------------------------------------------------------------------------
 // Philox4x32-10 counter-based generator (J. K. Salmon, M. A. Moraes, R. O. Dror,
 // D. E. Shaw, "Parallel Random Numbers: As Easy as 1, 2, 3", SC 2011) and a
-// Box-Muller transform to standard normals. Used for the fresh target noise of
+// Box-Muller transform to standard normals (four per call). Used for the fresh target noise of
 // the multi-plane loss; the oracle restates the same generator.
 // ---------------------------------------------------------------------------
 struct Philox4 {
@@ -109,15 +109,17 @@ __device__ __forceinline__ float u32_to_open01(uint32_t u) {
     return (float)(((double)u + 1.0) * 2.3283064365386963e-10);
 }
 
-// One standard normal for element `idx` of stream (`seed`, `offset`).
-// Box-Muller on the first two Philox words: z = sqrt(-2 ln u1) cos(2 pi u2).
-__device__ __forceinline__ float normal_at(uint64_t seed, uint64_t offset, uint64_t idx) {
-    Philox4 r = philox4x32_10((uint32_t)idx, (uint32_t)(idx >> 32), (uint32_t)offset, (uint32_t)(offset >> 32),
+// Four standard normals for counter `q` of stream (`seed`, `offset`): Box-Muller
+// on the word pairs (w0, w1) and (w2, w3), z = sqrt(-2 ln u) * (cos, sin)(2 pi u').
+__device__ __forceinline__ float4 normal4_at(uint64_t seed, uint64_t offset, uint64_t q) {
+    Philox4 r = philox4x32_10((uint32_t)q, (uint32_t)(q >> 32), (uint32_t)offset, (uint32_t)(offset >> 32),
                               (uint32_t)seed, (uint32_t)(seed >> 32));
-    const float u1 = u32_to_open01(r.v[0]);
-    const float u2 = u32_to_open01(r.v[1]);
-    const float rad = sqrtf(-2.0f * logf(u1));
-    return rad * cospif(2.0f * u2);
+    const float r01 = sqrtf(-2.0f * logf(u32_to_open01(r.v[0])));
+    const float r23 = sqrtf(-2.0f * logf(u32_to_open01(r.v[2])));
+    float s1, c1, s3, c3;
+    sincospif(2.0f * u32_to_open01(r.v[1]), &s1, &c1);
+    sincospif(2.0f * u32_to_open01(r.v[3]), &s3, &c3);
+    return make_float4(r01 * c1, r01 * s1, r23 * c3, r23 * s3);
 }
 
 }  // namespace cvqpg

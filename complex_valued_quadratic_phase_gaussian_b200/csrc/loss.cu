@@ -16,6 +16,9 @@
 // block, filters it separably (11 taps, sigma 1.5, valid), forms the SSIM map
 // and its three partial-derivative maps on the 42x42 map positions that touch
 // the tile, then applies the transposed filter to get dSSIM/dpred on the tile.
+// Every filter pass is register-blocked: a thread produces a run of 4-8
+// consecutive outputs along the filter direction from one sliding window of
+// inputs, so shared-memory reads per output drop from 11 to about 2.5.
 // Per-CTA partial sums (weighted L2, plain MSE, SSIM map sum) go to a fixed
 // slot; a finalize kernel reduces them in a fixed order (deterministic).
 #include "loss.cuh"
@@ -26,6 +29,22 @@ constexpr int kLT = 32;              // owned tile edge
 constexpr int kLH = kLT + 20;        // staged block edge (52)
 constexpr int kLM = kLT + 10;        // map positions touching the tile (42)
 constexpr int kLossThreads = 256;
+// shared-memory row strides, odd so that threads walking down a column hit distinct banks
+constexpr int kSXLd = kLH + 1;       // staged pred / target [52][53]
+constexpr int kHMLd = kLM + 1;       // horizontal moments [52][43] and SSIM partial maps [42][43]
+constexpr int kTMLd = kLT + 1;       // transposed-horizontal results [42][33]
+// outputs per thread in each pass
+constexpr int kHSeg = 7;             // horizontal moments: 52 rows x (42 = 6 x 7) columns
+constexpr int kVSeg = 7;             // vertical moments + SSIM: 42 columns x (42 = 6 x 7) rows
+constexpr int kTHSeg = 8;            // transposed horizontal: 42 rows x (32 = 4 x 8) columns
+constexpr int kTVSeg = 4;            // transposed vertical: 32 columns x (32 = 8 x 4) rows, one Philox call
+constexpr int kRegionA = 2 * kLH * kSXLd;  // sX, sY; later the three SSIM partial maps
+constexpr int kRegionB = 5 * kLH * kHMLd;  // five moment maps; later the transposed-horizontal maps
+static_assert(3 * kLM * kHMLd <= kRegionA, "SSIM partial maps must fit in the staging region");
+static_assert(3 * kLM * kTMLd <= kRegionB, "transposed maps must fit in the moment region");
+static_assert((kLM / kVSeg) * kLM <= kLossThreads, "one vertical item per thread");
+static_assert((kLT / kTHSeg) * kLM <= kLossThreads, "one transposed-horizontal item per thread");
+static_assert((kLT / kTVSeg) * kLT == kLossThreads, "one transposed-vertical item per thread");
 
 // Gaussian window, 11 taps, sigma 1.5, normalised (computed in double, rounded once).
 __device__ __forceinline__ float ssim_w(int k) {
@@ -35,19 +54,19 @@ __device__ __forceinline__ float ssim_w(int k) {
     return w[k];
 }
 
-__global__ void __launch_bounds__(kLossThreads) loss_kernel(LossDev L, const float* __restrict__ pred,
-                                                             const float* __restrict__ target,
-                                                             const uint8_t* __restrict__ depth_plane,
-                                                             const float* __restrict__ noise_scale,
-                                                             const int* __restrict__ iteration,
-                                                             float* __restrict__ grad_pred,
-                                                             float* __restrict__ partials) {
+__global__ void __launch_bounds__(kLossThreads, 3) loss_kernel(LossDev L, const float* __restrict__ pred,
+                                                                const float* __restrict__ target,
+                                                                const uint8_t* __restrict__ depth_plane,
+                                                                const float* __restrict__ noise_scale,
+                                                                const int* __restrict__ iteration,
+                                                                float* __restrict__ grad_pred,
+                                                                float* __restrict__ partials) {
     extern __shared__ float lsm[];
-    float* sX = lsm;                       // [52][52]
-    float* sY = sX + kLH * kLH;            // [52][52]
-    float* hM = sY + kLH * kLH;            // 5 maps [52][42]
-    float* dM = hM + 5 * kLH * kLM;        // 3 maps [42][42]
-    float* tM = sX;                        // 3 maps [42][32], reuses sX/sY/hM space after use
+    float* sX = lsm;                       // [52][53]
+    float* sY = sX + kLH * kSXLd;          // [52][53]
+    float* dM = lsm;                       // 3 x [42][43], written once sX/sY are dead
+    float* hM = lsm + kRegionA;            // 5 x [52][43]
+    float* tM = hM;                        // 3 x [42][33], written once hM is dead
     __shared__ float red[3][kLossThreads / 32];
 
     const int H = L.H, W = L.W;
@@ -59,119 +78,184 @@ __global__ void __launch_bounds__(kLossThreads) loss_kernel(LossDev L, const flo
     const size_t plane_off = (size_t)pc * H * W;
     const float* X = pred + plane_off;
     const float* Y = target + plane_off;
+    const int tid = threadIdx.x;
 
     // 1. stage the 52x52 block (zeros outside the image; never used by valid map entries)
-    for (int i = threadIdx.x; i < kLH * kLH; i += blockDim.x) {
+    for (int i = tid; i < kLH * kLH; i += kLossThreads) {
         const int r = i / kLH, q = i - r * kLH;
         const int y = y0 - 10 + r, x = x0 - 10 + q;
         const bool in = (unsigned)y < (unsigned)H && (unsigned)x < (unsigned)W;
-        sX[i] = in ? __ldg(&X[(size_t)y * W + x]) : 0.f;
-        sY[i] = in ? __ldg(&Y[(size_t)y * W + x]) : 0.f;
+        sX[r * kSXLd + q] = in ? __ldg(&X[(size_t)y * W + x]) : 0.f;
+        sY[r * kSXLd + q] = in ? __ldg(&Y[(size_t)y * W + x]) : 0.f;
     }
     __syncthreads();
-    // 2. horizontal filter -> 5 moment maps on [52][42]
-    for (int i = threadIdx.x; i < kLH * kLM; i += blockDim.x) {
-        const int r = i / kLM, q = i - r * kLM;
-        float a = 0.f, b = 0.f, aa = 0.f, bb = 0.f, ab = 0.f;
+
+    // 2. horizontal filter -> moments x, y, xx, yy, xy on [52][42]; item = (row, 7 columns)
+    for (int item = tid; item < kLH * (kLM / kHSeg); item += kLossThreads) {
+        const int r = item % kLH, c0 = (item / kLH) * kHSeg;
+        float acc[5][kHSeg];
 #pragma unroll
-        for (int k = 0; k < 11; k++) {
-            const float w = ssim_w(k), x = sX[r * kLH + q + k], y = sY[r * kLH + q + k];
-            a = fmaf(w, x, a);
-            b = fmaf(w, y, b);
-            aa = fmaf(w, x * x, aa);
-            bb = fmaf(w, y * y, bb);
-            ab = fmaf(w, x * y, ab);
+        for (int o = 0; o < kHSeg; o++)
+#pragma unroll
+            for (int m = 0; m < 5; m++) acc[m][o] = 0.f;
+        const float* px = sX + r * kSXLd + c0;
+        const float* py = sY + r * kSXLd + c0;
+#pragma unroll
+        for (int k = 0; k < kHSeg + 10; k++) {
+            const float x = px[k], y = py[k];
+            const float xx = x * x, yy = y * y, xy = x * y;
+#pragma unroll
+            for (int o = 0; o < kHSeg; o++) {
+                const int t = k - o;
+                if (t < 0 || t > 10) continue;
+                const float w = ssim_w(t);
+                acc[0][o] = fmaf(w, x, acc[0][o]);
+                acc[1][o] = fmaf(w, y, acc[1][o]);
+                acc[2][o] = fmaf(w, xx, acc[2][o]);
+                acc[3][o] = fmaf(w, yy, acc[3][o]);
+                acc[4][o] = fmaf(w, xy, acc[4][o]);
+            }
         }
-        hM[0 * kLH * kLM + i] = a;
-        hM[1 * kLH * kLM + i] = b;
-        hM[2 * kLH * kLM + i] = aa;
-        hM[3 * kLH * kLM + i] = bb;
-        hM[4 * kLH * kLM + i] = ab;
+#pragma unroll
+        for (int m = 0; m < 5; m++)
+#pragma unroll
+            for (int o = 0; o < kHSeg; o++) hM[m * kLH * kHMLd + r * kHMLd + c0 + o] = acc[m][o];
     }
     __syncthreads();
-    // 3. vertical filter -> SSIM map and its partials on the valid map positions
+
+    // 3. vertical filter -> SSIM map and its partials on [42][42]; item = (column, 7 rows)
     const float C1 = L.c1, C2 = L.c2;
     float ssim_sum = 0.f;
-    for (int i = threadIdx.x; i < kLM * kLM; i += blockDim.x) {
-        const int ii = i / kLM, jj = i - ii * kLM;
-        const int mi = y0 - 10 + ii, mj = x0 - 10 + jj;
-        float dm = 0.f, dxx = 0.f, dxy = 0.f;
-        if ((unsigned)mi < (unsigned)(H - 10) && (unsigned)mj < (unsigned)(W - 10)) {
-            float mu1 = 0.f, mu2 = 0.f, exx = 0.f, eyy = 0.f, exy = 0.f;
+    if (tid < kLM * (kLM / kVSeg)) {
+        const int jj = tid % kLM, i0 = (tid / kLM) * kVSeg;
+        float acc[5][kVSeg];
 #pragma unroll
-            for (int k = 0; k < 11; k++) {
-                const float w = ssim_w(k);
-                const int o = (ii + k) * kLM + jj;
-                mu1 = fmaf(w, hM[0 * kLH * kLM + o], mu1);
-                mu2 = fmaf(w, hM[1 * kLH * kLM + o], mu2);
-                exx = fmaf(w, hM[2 * kLH * kLM + o], exx);
-                eyy = fmaf(w, hM[3 * kLH * kLM + o], eyy);
-                exy = fmaf(w, hM[4 * kLH * kLM + o], exy);
+        for (int o = 0; o < kVSeg; o++)
+#pragma unroll
+            for (int m = 0; m < 5; m++) acc[m][o] = 0.f;
+#pragma unroll
+        for (int k = 0; k < kVSeg + 10; k++) {
+            float v[5];
+#pragma unroll
+            for (int m = 0; m < 5; m++) v[m] = hM[m * kLH * kHMLd + (i0 + k) * kHMLd + jj];
+#pragma unroll
+            for (int o = 0; o < kVSeg; o++) {
+                const int t = k - o;
+                if (t < 0 || t > 10) continue;
+                const float w = ssim_w(t);
+#pragma unroll
+                for (int m = 0; m < 5; m++) acc[m][o] = fmaf(w, v[m], acc[m][o]);
             }
-            const float s11 = exx - mu1 * mu1, s22 = eyy - mu2 * mu2, s12 = exy - mu1 * mu2;
-            const float A1 = 2.f * mu1 * mu2 + C1, A2 = 2.f * s12 + C2;
-            const float B1 = mu1 * mu1 + mu2 * mu2 + C1, B2 = s11 + s22 + C2;
-            const float iB1 = 1.f / B1, iB2 = 1.f / B2;
-            const float smap = A1 * A2 * iB1 * iB2;
-            if (ii >= 10 && jj >= 10) ssim_sum += smap;  // owned map position
-            dm = 2.f * mu2 * A2 * iB1 * iB2 - 2.f * mu1 * smap * iB1 + A1 * iB1 * (-2.f * mu2 * iB2 + 2.f * mu1 * A2 * iB2 * iB2);
-            dxx = -smap * iB2;
-            dxy = 2.f * A1 * iB1 * iB2;
         }
-        dM[0 * kLM * kLM + i] = dm;
-        dM[1 * kLM * kLM + i] = dxx;
-        dM[2 * kLM * kLM + i] = dxy;
-    }
-    __syncthreads();
-    // 4. transposed horizontal filter -> [42][32]
-    for (int i = threadIdx.x; i < kLM * kLT; i += blockDim.x) {
-        const int ii = i / kLT, xx = i - ii * kLT;
-        float a = 0.f, b = 0.f, c = 0.f;
+        const int mj = x0 - 10 + jj;
+        const bool col_ok = (unsigned)mj < (unsigned)(W - 10);
 #pragma unroll
-        for (int k = 0; k < 11; k++) {
-            const float w = ssim_w(k);
-            const int o = ii * kLM + xx + 10 - k;
-            a = fmaf(w, dM[0 * kLM * kLM + o], a);
-            b = fmaf(w, dM[1 * kLM * kLM + o], b);
-            c = fmaf(w, dM[2 * kLM * kLM + o], c);
+        for (int o = 0; o < kVSeg; o++) {
+            const int ii = i0 + o, mi = y0 - 10 + ii;
+            float dm = 0.f, dxx = 0.f, dxy = 0.f;
+            if (col_ok && (unsigned)mi < (unsigned)(H - 10)) {
+                const float mu1 = acc[0][o], mu2 = acc[1][o];
+                const float s11 = acc[2][o] - mu1 * mu1, s22 = acc[3][o] - mu2 * mu2, s12 = acc[4][o] - mu1 * mu2;
+                const float A1 = 2.f * mu1 * mu2 + C1, A2 = 2.f * s12 + C2;
+                const float B1 = mu1 * mu1 + mu2 * mu2 + C1, B2 = s11 + s22 + C2;
+                const float iB1 = 1.f / B1, iB2 = 1.f / B2;
+                const float smap = A1 * A2 * iB1 * iB2;
+                if (ii >= 10 && jj >= 10) ssim_sum += smap;  // owned map position
+                dm = 2.f * mu2 * A2 * iB1 * iB2 - 2.f * mu1 * smap * iB1 +
+                     A1 * iB1 * (-2.f * mu2 * iB2 + 2.f * mu1 * A2 * iB2 * iB2);
+                dxx = -smap * iB2;
+                dxy = 2.f * A1 * iB1 * iB2;
+            }
+            dM[0 * kLM * kHMLd + ii * kHMLd + jj] = dm;
+            dM[1 * kLM * kHMLd + ii * kHMLd + jj] = dxx;
+            dM[2 * kLM * kHMLd + ii * kHMLd + jj] = dxy;
         }
-        tM[0 * kLM * kLT + i] = a;
-        tM[1 * kLM * kLT + i] = b;
-        tM[2 * kLM * kLT + i] = c;
     }
     __syncthreads();
-    // 5. transposed vertical filter + L2 terms on the owned tile
+
+    // 4. transposed horizontal filter -> [42][32]; item = (row, 8 columns)
+    if (tid < kLM * (kLT / kTHSeg)) {
+        const int ii = tid % kLM, c0 = (tid / kLM) * kTHSeg;
+        float acc[3][kTHSeg];
+#pragma unroll
+        for (int o = 0; o < kTHSeg; o++)
+#pragma unroll
+            for (int m = 0; m < 3; m++) acc[m][o] = 0.f;
+#pragma unroll
+        for (int k = 0; k < kTHSeg + 10; k++) {
+            float v[3];
+#pragma unroll
+            for (int m = 0; m < 3; m++) v[m] = dM[m * kLM * kHMLd + ii * kHMLd + c0 + k];
+#pragma unroll
+            for (int o = 0; o < kTHSeg; o++) {
+                const int t = o + 10 - k;  // map column c0+k feeds tile column c0+o with weight w(o+10-k)
+                if (t < 0 || t > 10) continue;
+                const float w = ssim_w(t);
+#pragma unroll
+                for (int m = 0; m < 3; m++) acc[m][o] = fmaf(w, v[m], acc[m][o]);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+#pragma unroll
+            for (int o = 0; o < kTHSeg; o++) tM[m * kLM * kTMLd + ii * kTMLd + c0 + o] = acc[m][o];
+    }
+    __syncthreads();
+
+    // 5. transposed vertical filter + L2 terms on the owned tile; item = (column, 4 rows)
     const float inv_n = L.inv_n, ssim_scale = -L.ssim_weight * L.inv_nmap;
     const float nscale = noise_scale[p];
     const uint64_t it = iteration ? (uint64_t)(uint32_t)iteration[0] : 0ull;
     float l2_sum = 0.f, mse_sum = 0.f;
-    for (int i = threadIdx.x; i < kLT * kLT; i += blockDim.x) {
-        const int yy = i / kLT, xx = i - yy * kLT;
-        const int y = y0 + yy, x = x0 + xx;
-        if (y >= H || x >= W) continue;
-        float gm = 0.f, gxx = 0.f, gxy = 0.f;
+    {
+        const int xx = tid % kLT, r0 = (tid / kLT) * kTVSeg;
+        float acc[3][kTVSeg];
 #pragma unroll
-        for (int k = 0; k < 11; k++) {
-            const float w = ssim_w(k);
-            const int o = (yy + 10 - k) * kLT + xx;
-            gm = fmaf(w, tM[0 * kLM * kLT + o], gm);
-            gxx = fmaf(w, tM[1 * kLM * kLT + o], gxx);
-            gxy = fmaf(w, tM[2 * kLM * kLT + o], gxy);
+        for (int o = 0; o < kTVSeg; o++)
+#pragma unroll
+            for (int m = 0; m < 3; m++) acc[m][o] = 0.f;
+#pragma unroll
+        for (int k = 0; k < kTVSeg + 10; k++) {
+            float v[3];
+#pragma unroll
+            for (int m = 0; m < 3; m++) v[m] = tM[m * kLM * kTMLd + (r0 + k) * kTMLd + xx];
+#pragma unroll
+            for (int o = 0; o < kTVSeg; o++) {
+                const int t = o + 10 - k;
+                if (t < 0 || t > 10) continue;
+                const float w = ssim_w(t);
+#pragma unroll
+                for (int m = 0; m < 3; m++) acc[m][o] = fmaf(w, v[m], acc[m][o]);
+            }
         }
-        const size_t e = (size_t)y * W + x;
-        const float xv = __ldg(&X[e]), tv = __ldg(&Y[e]);
-        const float m = (__ldg(&depth_plane[e]) == p) ? 1.f : 0.f;
-        float nv = tv;
-        if (L.inject_noise) {
-            const float z = normal_at(L.seed, it, plane_off + e);
-            nv = tv + (z * L.noise_ratio) * nscale;
+        const int x = x0 + xx, yb = y0 + r0;
+        if (x < W && yb < H) {
+            float z[kTVSeg] = {0.f, 0.f, 0.f, 0.f};
+            if (L.inject_noise) {
+                // counter of the four rows yb..yb+3 of column x (yb is a multiple of 4)
+                const uint64_t q = ((uint64_t)pc * (uint64_t)((H + 3) >> 2) + (uint64_t)(yb >> 2)) * (uint64_t)W + x;
+                const float4 n4 = normal4_at(L.seed, it, q);
+                z[0] = n4.x;
+                z[1] = n4.y;
+                z[2] = n4.z;
+                z[3] = n4.w;
+            }
+#pragma unroll
+            for (int o = 0; o < kTVSeg; o++) {
+                const int y = yb + o;
+                if (y >= H) break;
+                const size_t e = (size_t)y * W + x;
+                const float xv = __ldg(&X[e]), tv = __ldg(&Y[e]);
+                const float m = (__ldg(&depth_plane[e]) == p) ? 1.f : 0.f;
+                const float nv = L.inject_noise ? tv + (z[o] * L.noise_ratio) * nscale : tv;
+                const float d0 = xv - tv, d1 = (xv * m - nv * m), d2 = (xv * nv - nv * nv);
+                l2_sum += L.w0 * d0 * d0 + L.w1 * d1 * d1 + L.w2 * d2 * d2;
+                mse_sum += d0 * d0;
+                const float g_l2 = 2.f * inv_n * (L.w0 * d0 + L.w1 * d1 * m + L.w2 * d2 * nv);
+                const float g_ssim = ssim_scale * (acc[0][o] + 2.f * xv * acc[1][o] + tv * acc[2][o]);
+                grad_pred[plane_off + e] = g_l2 + g_ssim;
+            }
         }
-        const float d0 = xv - tv, d1 = (xv * m - nv * m), d2 = (xv * nv - nv * nv);
-        l2_sum += L.w0 * d0 * d0 + L.w1 * d1 * d1 + L.w2 * d2 * d2;
-        mse_sum += d0 * d0;
-        const float g_l2 = 2.f * inv_n * (L.w0 * d0 + L.w1 * d1 * m + L.w2 * d2 * nv);
-        const float g_ssim = ssim_scale * (gm + 2.f * xv * gxx + tv * gxy);
-        grad_pred[plane_off + e] = g_l2 + g_ssim;
     }
     // 6. block reduction of the three partial sums
 #pragma unroll
@@ -180,14 +264,14 @@ __global__ void __launch_bounds__(kLossThreads) loss_kernel(LossDev L, const flo
         mse_sum += __shfl_xor_sync(0xffffffffu, mse_sum, o);
         ssim_sum += __shfl_xor_sync(0xffffffffu, ssim_sum, o);
     }
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = tid >> 5, lane = tid & 31;
     if (lane == 0) {
         red[0][w] = l2_sum;
         red[1][w] = mse_sum;
         red[2][w] = ssim_sum;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         float a = 0.f, b = 0.f, c = 0.f;
         for (int k = 0; k < kLossThreads / 32; k++) {
             a += red[0][k];
@@ -201,53 +285,73 @@ __global__ void __launch_bounds__(kLossThreads) loss_kernel(LossDev L, const flo
     }
 }
 
-// out[0] = total loss, out[1 + p] = MSE of plane p, out[1 + P + p] = SSIM of plane p,
-// out[1 + 2P + p] = loss of plane p. Fixed-order double accumulation.
-__global__ void loss_finalize_kernel(LossDev L, const float* __restrict__ partials, float* __restrict__ out) {
-    const int tiles = ((L.W + kLT - 1) / kLT) * ((L.H + kLT - 1) / kLT);
-    __shared__ double acc[kMaxLossPlanes][3];
-    const int p = threadIdx.x;
-    if (p < L.P) {
-        double a = 0.0, b = 0.0, c = 0.0;
-        for (int ch = 0; ch < L.C; ch++)
-            for (int t = 0; t < tiles; t++) {
-                const float* s = partials + ((size_t)(p * L.C + ch) * tiles + t) * 3;
-                a += s[0];
-                b += s[1];
-                c += s[2];
-            }
-        acc[p][0] = a;
-        acc[p][1] = b;
-        acc[p][2] = c;
-    }
+// Fixed-order block sum of one double per thread (blockDim.x == kFinalThreads).
+constexpr int kFinalThreads = 1024;
+constexpr int kRangeThreads = 512;
+constexpr int kRangeBlocks = CVQPG_TARGET_RANGE_WORKSPACE_PER_PLANE / 8;  // (max, min) float pairs
+
+__device__ __forceinline__ double block_sum_fixed(double v, double* sh) {
+    sh[threadIdx.x] = v;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double total = 0.0;
-        for (int q = 0; q < L.P; q++) {
-            const double mse = acc[q][1] * L.inv_n;
-            const double ssim = acc[q][2] * L.inv_nmap;
-            const double lp = acc[q][0] * L.inv_n + L.ssim_weight * (1.0 - ssim);
+#pragma unroll 1
+    for (int s = kFinalThreads / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// out[0] = total loss, out[1 + p] = MSE of plane p, out[1 + P + p] = SSIM of plane p,
+// out[1 + 2P + p] = loss of plane p. One block; each thread accumulates a fixed
+// strided subset of the per-tile partials in double, then a fixed-shape tree
+// adds the threads, so the result does not depend on scheduling.
+__global__ void __launch_bounds__(kFinalThreads) loss_finalize_kernel(LossDev L, const float* __restrict__ partials,
+                                                                      float* __restrict__ out) {
+    __shared__ double sh[kFinalThreads];
+    const int per_plane = L.C * ((L.W + kLT - 1) / kLT) * ((L.H + kLT - 1) / kLT);
+    double total = 0.0;
+    for (int q = 0; q < L.P; q++) {
+        double a = 0.0, b = 0.0, c = 0.0;
+        const float* base = partials + (size_t)q * per_plane * 3;
+        for (int t = threadIdx.x; t < per_plane; t += kFinalThreads) {
+            a += base[(size_t)t * 3 + 0];
+            b += base[(size_t)t * 3 + 1];
+            c += base[(size_t)t * 3 + 2];
+        }
+        a = block_sum_fixed(a, sh);
+        b = block_sum_fixed(b, sh);
+        c = block_sum_fixed(c, sh);
+        const double mse = b * L.inv_n;
+        const double ssim = c * L.inv_nmap;
+        const double lp = a * L.inv_n + L.ssim_weight * (1.0 - ssim);
+        total += lp;
+        if (threadIdx.x == 0) {
             out[1 + q] = (float)mse;
             out[1 + L.P + q] = (float)ssim;
             out[1 + 2 * L.P + q] = (float)lp;
-            total += lp;
         }
-        out[0] = (float)total;
     }
+    if (threadIdx.x == 0) out[0] = (float)total;
 }
 
-// per-plane noise scale: ratio applied later; here max(T_p) - min(T_p)
-__global__ void target_range_kernel(const float* __restrict__ targets, size_t plane_elems,
-                                     float* __restrict__ range_out) {
-    const int p = blockIdx.x;
+// Per-plane noise scale max(T_p) - min(T_p) (the ratio is applied later).
+// Pass 1, grid (kRangeBlocks, planes): each block reduces a strided slice of
+// its plane to (max, min). Pass 2, one warp per plane: combine the slices.
+__global__ void __launch_bounds__(kRangeThreads) target_range_slices_kernel(const float* __restrict__ targets,
+                                                                            size_t plane_elems,
+                                                                            float2* __restrict__ slices) {
+    const int p = blockIdx.y;
     const float* t = targets + (size_t)p * plane_elems;
     float mx = -INFINITY, mn = INFINITY;
-    for (size_t i = threadIdx.x; i < plane_elems; i += blockDim.x) {
-        const float v = t[i];
+    for (size_t i = (size_t)blockIdx.x * kRangeThreads + threadIdx.x; i < plane_elems;
+         i += (size_t)kRangeBlocks * kRangeThreads) {
+        const float v = __ldg(&t[i]);
         mx = fmaxf(mx, v);
         mn = fminf(mn, v);
     }
-    __shared__ float smx[32], smn[32];
+    __shared__ float smx[kRangeThreads / 32], smn[kRangeThreads / 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -259,12 +363,28 @@ __global__ void target_range_kernel(const float* __restrict__ targets, size_t pl
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
+        for (int k = 1; k < kRangeThreads / 32; k++) {
             mx = fmaxf(mx, smx[k]);
             mn = fminf(mn, smn[k]);
         }
-        range_out[p] = fmaxf(mx, smx[0]) - fminf(mn, smn[0]);
+        slices[(size_t)p * kRangeBlocks + blockIdx.x] = make_float2(mx, mn);
     }
+}
+
+__global__ void target_range_combine_kernel(const float2* __restrict__ slices, float* __restrict__ range_out) {
+    const int p = blockIdx.x;
+    float mx = -INFINITY, mn = INFINITY;
+    for (int k = threadIdx.x; k < kRangeBlocks; k += 32) {
+        const float2 v = slices[(size_t)p * kRangeBlocks + k];
+        mx = fmaxf(mx, v.x);
+        mn = fminf(mn, v.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    if (threadIdx.x == 0) range_out[p] = mx - mn;
 }
 
 int loss_make_dev(const cvqpg_loss_params* q, LossDev* L) {
@@ -295,10 +415,7 @@ size_t loss_partials_floats(const LossDev& L) {
     return (size_t)L.P * L.C * tiles * 3;
 }
 
-static size_t loss_smem() {
-    const size_t a = (size_t)(2 * kLH * kLH + 5 * kLH * kLM + 3 * kLM * kLM) * sizeof(float);
-    return a;
-}
+static size_t loss_smem() { return (size_t)(kRegionA + kRegionB) * sizeof(float); }
 
 void launch_loss(const LossDev& L, const float* pred, const float* targets, const uint8_t* depth_plane,
                  const float* noise_scale, const int* iteration, float* grad_pred, float* partials, float* out,
@@ -308,12 +425,15 @@ void launch_loss(const LossDev& L, const float* pred, const float* targets, cons
     cudaFuncSetAttribute(loss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     loss_kernel<<<L.P * L.C * tiles, kLossThreads, sm, stream>>>(L, pred, targets, depth_plane, noise_scale,
                                                                  iteration, grad_pred, partials);
-    loss_finalize_kernel<<<1, 32, 0, stream>>>(L, partials, out);
+    loss_finalize_kernel<<<1, kFinalThreads, 0, stream>>>(L, partials, out);
 }
 
-void launch_target_range(const float* targets, int planes, size_t plane_elems, float* range_out,
+void launch_target_range(const float* targets, int planes, size_t plane_elems, float* range_out, void* scratch,
                          cudaStream_t stream) {
-    target_range_kernel<<<planes, 1024, 0, stream>>>(targets, plane_elems, range_out);
+    float2* slices = (float2*)scratch;
+    target_range_slices_kernel<<<dim3(kRangeBlocks, planes), kRangeThreads, 0, stream>>>(targets, plane_elems,
+                                                                                         slices);
+    target_range_combine_kernel<<<planes, 32, 0, stream>>>(slices, range_out);
 }
 
 }  // namespace cvqpg
@@ -328,14 +448,19 @@ extern "C" int cvqpg_loss_workspace_size(const cvqpg_loss_params* q, size_t* byt
     LossDev L;
     const int st = loss_make_dev(q, &L);
     if (st != CVQPG_OK) return st;
-    *bytes = loss_partials_floats(L) * sizeof(float) + 256;
+    const size_t partials = loss_partials_floats(L) * sizeof(float);
+    const size_t range = (size_t)L.P * CVQPG_TARGET_RANGE_WORKSPACE_PER_PLANE;
+    *bytes = (partials > range ? partials : range) + 256;
     return CVQPG_OK;
 }
 
 extern "C" int cvqpg_loss_target_range(const float* targets, int planes, int channels, int height, int width,
-                                       float* range_out, void* stream) {
-    if (!targets || !range_out || planes < 1 || channels < 1 || height < 1 || width < 1) return CVQPG_ERR_ARG;
-    launch_target_range(targets, planes, (size_t)channels * height * width, range_out, (cudaStream_t)stream);
+                                       float* range_out, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!targets || !range_out || !workspace || planes < 1 || channels < 1 || height < 1 || width < 1)
+        return CVQPG_ERR_ARG;
+    if (workspace_bytes < (size_t)planes * CVQPG_TARGET_RANGE_WORKSPACE_PER_PLANE) return CVQPG_ERR_WORKSPACE;
+    launch_target_range(targets, planes, (size_t)channels * height * width, range_out, workspace,
+                        (cudaStream_t)stream);
     return launch_status();
 }
 

@@ -23,7 +23,7 @@ size_t loss_partials_floats(const LossDev& L);
 void launch_loss(const LossDev& L, const float* pred, const float* targets, const uint8_t* depth_plane,
                  const float* noise_scale, const int* iteration, float* grad_pred, float* partials, float* out,
                  cudaStream_t stream);
-void launch_target_range(const float* targets, int planes, size_t plane_elems, float* range_out,
+void launch_target_range(const float* targets, int planes, size_t plane_elems, float* range_out, void* scratch,
                          cudaStream_t stream);
 
 }  // namespace cvqpg

@@ -22,6 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .loss import TARGET_RANGE_WORKSPACE_PER_PLANE
 from .propagator import reference_distances, reference_pad_size
 
 CULL_CUDA16_5SIGMA = 0
@@ -230,8 +231,10 @@ class Fitter:
             if tuple(self.targets.shape) != (P, C, H, W) or tuple(self.depth_plane.shape) != (H, W):
                 raise ValueError("targets must be [P,C,H,W] and depth_plane [H,W]")
             self.target_range = torch.empty(P, dtype=torch.float32, device=self.device)
+            scratch = _lib.workspace(P * TARGET_RANGE_WORKSPACE_PER_PLANE, self.device)
             _lib.check(lib.cvqpg_loss_target_range(_lib.ptr(self.targets), P, C, H, W, _lib.ptr(self.target_range),
-                                                   _lib.stream_of(self.device)), "cvqpg_loss_target_range")
+                                                   _lib.ptr(scratch), scratch.numel(), _lib.stream_of(self.device)),
+                       "cvqpg_loss_target_range")
         if init is None:
             init = synthetic_init(cfg, cfg.seed)
         self.load_raw(init)

@@ -3,7 +3,9 @@
     python -m complex_valued_quadratic_phase_gaussian_b200.stagebench --stage blasm_fwd --workload rgb1080 --iters 3
 
 Stages: ``blasm_fwd`` (rows, columns, inverse rows), ``blasm_adj`` (the three
-adjoint passes), ``render`` (binning + splat forward of the drop-in path).
+adjoint passes), ``render`` (binning + splat forward of the drop-in path),
+``splat_adj`` (the splat adjoint alone, on the lists of one forward call),
+``loss`` (multi-plane loss + SSIM forward and dL/d(pred), with target noise).
 Only the buffers of that stage are allocated, so the process stays small
 enough for kernel-level profiling. Prints one JSON line with the mean
 milliseconds per call (CUDA events on the launching stream).
@@ -54,8 +56,8 @@ def run(stage, workload, iters=3, warmup=1):
             torch.cuda.synchronize()
             if i >= warmup:
                 times.append(s.elapsed_time(e))
-    elif stage == "render":
-        from .rasterizer import render_forward
+    elif stage in ("render", "splat_adj"):
+        from .rasterizer import render_backward, render_forward
         rng = np.random.default_rng(0)
         N = w["N"]
         means = torch.from_numpy(np.stack([rng.uniform(0, W, N), rng.uniform(0, H, N)], 1).astype(np.float32)).cuda()
@@ -65,10 +67,33 @@ def run(stage, workload, iters=3, warmup=1):
         z = torch.rand(N, device="cuda")
         radii = torch.full((N,), 12, dtype=torch.int32, device="cuda")
         k = (2 * np.pi / torch.tensor(w["wl"], dtype=torch.float32)).cuda()
+        args = (means, inv, col, ph, z, z * 500, z + 4, k)
+        _, pl, ranges = render_forward(*args, w["pitch"] ** 2, W, H, radii=radii)
+        g = _field(C, H, W, seed=2)
         for i in range(warmup + iters):
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record()
-            render_forward(means, inv, col, ph, z, z * 500, z + 4, k, w["pitch"] ** 2, W, H, radii=radii)
+            if stage == "render":
+                render_forward(*args, w["pitch"] ** 2, W, H, radii=radii)
+            else:
+                render_backward(g, *args, pl, ranges, w["pitch"] ** 2, W, H)
+            e.record()
+            torch.cuda.synchronize()
+            if i >= warmup:
+                times.append(s.elapsed_time(e))
+    elif stage == "loss":
+        from .loss import MultiplaneLoss
+        gen = torch.Generator(device="cuda").manual_seed(0)
+        targets = torch.rand((P, C, H, W), device="cuda", generator=gen)
+        pred = (0.9 * targets + 0.1 * torch.rand((P, C, H, W), device="cuda", generator=gen)).clamp_(0, 1)
+        depth = torch.randint(0, P, (H, W), device="cuda", generator=gen, dtype=torch.int32).to(torch.uint8)
+        lf = MultiplaneLoss(targets, depth, seed=1)
+        out, grad = lf(pred, iteration=0)
+        it = torch.zeros(1, dtype=torch.int32, device="cuda")
+        for i in range(warmup + iters):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            lf(pred, iteration=it, out=out, grad_pred=grad)
             e.record()
             torch.cuda.synchronize()
             if i >= warmup:
@@ -80,7 +105,7 @@ def run(stage, workload, iters=3, warmup=1):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--stage", default="blasm_fwd", choices=["blasm_fwd", "blasm_adj", "render"])
+    ap.add_argument("--stage", default="blasm_fwd", choices=["blasm_fwd", "blasm_adj", "render", "splat_adj", "loss"])
     ap.add_argument("--workload", default="rgb1080", choices=sorted(WORKLOADS))
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)

@@ -239,9 +239,12 @@ typedef struct cvqpg_loss_params {
 } cvqpg_loss_params;
 
 CVQPG_API int cvqpg_loss_workspace_size(const cvqpg_loss_params* prm, size_t* bytes);
-/* target_range[p] = max(T_p) - min(T_p), once per fit (targets are constant). */
+/* target_range[p] = max(T_p) - min(T_p), once per fit (targets are constant).
+ * workspace: at least planes * CVQPG_TARGET_RANGE_WORKSPACE_PER_PLANE bytes
+ * (the cvqpg_loss_workspace_size workspace of the same planes is enough). */
+#define CVQPG_TARGET_RANGE_WORKSPACE_PER_PLANE 512
 CVQPG_API int cvqpg_loss_target_range(const float* targets, int planes, int channels, int height, int width,
-                                      float* target_range, void* stream);
+                                      float* target_range, void* workspace, size_t workspace_bytes, void* stream);
 CVQPG_API int cvqpg_loss_forward_backward(const cvqpg_loss_params* prm, const float* pred, const float* targets,
                                           const uint8_t* depth_plane, const float* target_range,
                                           const int32_t* iteration, float* grad_pred, float* out,

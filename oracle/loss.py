@@ -35,41 +35,51 @@ def philox4x32_10(c0, c1, c2, c3, k0, k1):
     return c
 
 
-def normal_at(seed, offset, idx):
-    """Standard normals for element indices idx of stream (seed, offset), float32 Box-Muller."""
-    idx = np.asarray(idx, dtype=np.uint64)
+def normals4_at(seed, offset, q):
+    """Four standard normals per counter q of stream (seed, offset): float32 Box-Muller on the
+    Philox word pairs (w0, w1) and (w2, w3). Returns float32 [..., 4]."""
+    q = np.asarray(q, dtype=np.uint64)
     seed, offset = int(seed), int(offset)
-    r = philox4x32_10(idx & M32, idx >> np.uint64(32), offset & 0xFFFFFFFF, (offset >> 32) & 0xFFFFFFFF,
+    r = philox4x32_10(q & M32, q >> np.uint64(32), offset & 0xFFFFFFFF, (offset >> 32) & 0xFFFFFFFF,
                       seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
-    u1 = ((r[0].astype(np.float64) + 1.0) * 2.3283064365386963e-10).astype(np.float32)
-    u2 = ((r[1].astype(np.float64) + 1.0) * 2.3283064365386963e-10).astype(np.float32)
-    rad = np.sqrt(np.float32(-2.0) * np.log(u1))
-    return (rad * np.cos(np.float32(2.0 * np.pi) * u2)).astype(np.float32)
+    u = [((w.astype(np.float64) + 1.0) * 2.3283064365386963e-10).astype(np.float32) for w in r]
+    two_pi = np.float32(2.0 * np.pi)
+    r01 = np.sqrt(np.float32(-2.0) * np.log(u[0]))
+    r23 = np.sqrt(np.float32(-2.0) * np.log(u[2]))
+    a1, a3 = two_pi * u[1], two_pi * u[3]
+    return np.stack([r01 * np.cos(a1), r01 * np.sin(a1), r23 * np.cos(a3), r23 * np.sin(a3)], -1).astype(np.float32)
 
 
 def plane_noise(shape, seed, iteration):
-    """Noise tensor [P,C,H,W] for one iteration (element index = flat index)."""
-    n = int(np.prod(shape))
-    return normal_at(seed, iteration, np.arange(n, dtype=np.uint64)).reshape(shape)
+    """Noise tensor [P,C,H,W] for one iteration.
+
+    Element (image i = p*C + c, row y, column x) takes normal (y % 4) of counter
+    q = (i * ceil(H/4) + y // 4) * W + x, so four vertically adjacent pixels
+    share one Philox call.
+    """
+    P, C, H, W = shape
+    Hq = (H + 3) // 4
+    q = np.arange(P * C * Hq * W, dtype=np.uint64)
+    n4 = normals4_at(seed, iteration, q).reshape(P * C, Hq, W, 4)
+    z = n4.transpose(0, 1, 3, 2).reshape(P * C, Hq * 4, W)[:, :H, :]
+    return np.ascontiguousarray(z).reshape(P, C, H, W)
 
 
-def multiplane_loss(V, targets, depth_plane, weights=(1.0, 1.0, 1.0), ssim_weight=0.005, noise=None,
-                    noise_ratio=1e-3):
-    """Loss over all planes and dL/dV (torch convention). V [P,C,H,W] complex.
+def multiplane_loss_pred(pred, targets, depth_plane, weights=(1.0, 1.0, 1.0), ssim_weight=0.005, noise=None,
+                         noise_ratio=1e-3):
+    """Loss over all planes of the clamped intensity pred [P,C,H,W] and dL/d(pred).
 
     noise: None (no injection) or standard normals [P,C,H,W].
-    Returns (loss, per-plane MSE, per-plane SSIM, grad_V).
+    Returns (loss, per-plane MSE, per-plane SSIM, per-plane loss, grad_pred).
     """
-    V = np.asarray(V, dtype=np.complex128)
+    pred = np.asarray(pred, dtype=np.float64)
     T = np.asarray(targets, dtype=np.float64)
-    P, C, H, W = V.shape
-    I = np.abs(V) ** 2
-    pred = np.clip(I, 0.0, 1.0)
+    P, C, H, W = pred.shape
     n = C * H * W
     w0, w1, w2 = weights
     total = 0.0
-    mses, ssims = [], []
-    gI = np.zeros_like(I)
+    mses, ssims, losses = [], [], []
+    gx = np.zeros_like(pred)
     for p in range(P):
         x, t = pred[p], T[p]
         m = (np.asarray(depth_plane) == p).astype(np.float64)[None].repeat(C, 0)
@@ -81,13 +91,29 @@ def multiplane_loss(V, targets, depth_plane, weights=(1.0, 1.0, 1.0), ssim_weigh
         d0, d1, d2 = x - t, x * m - nt * m, x * nt - nt * nt
         l2 = (w0 * (d0 ** 2).sum() + w1 * (d1 ** 2).sum() + w2 * (d2 ** 2).sum()) / n
         s, gs = ossim.ssim_value_and_grad(x, t)
-        total += l2 + ssim_weight * (1.0 - s)
+        lp = l2 + ssim_weight * (1.0 - s)
+        total += lp
         mses.append((d0 ** 2).mean())
         ssims.append(s)
-        gx = 2.0 / n * (w0 * d0 + w1 * d1 * m + w2 * d2 * nt) - ssim_weight * gs
-        gI[p] = np.where(I[p] <= 1.0, gx, 0.0)
+        losses.append(lp)
+        gx[p] = 2.0 / n * (w0 * d0 + w1 * d1 * m + w2 * d2 * nt) - ssim_weight * gs
+    return total, np.array(mses), np.array(ssims), np.array(losses), gx
+
+
+def multiplane_loss(V, targets, depth_plane, weights=(1.0, 1.0, 1.0), ssim_weight=0.005, noise=None,
+                    noise_ratio=1e-3):
+    """Loss over all planes and dL/dV (torch convention). V [P,C,H,W] complex.
+
+    noise: None (no injection) or standard normals [P,C,H,W].
+    Returns (loss, per-plane MSE, per-plane SSIM, grad_V).
+    """
+    V = np.asarray(V, dtype=np.complex128)
+    I = np.abs(V) ** 2
+    total, mses, ssims, _, gx = multiplane_loss_pred(np.clip(I, 0.0, 1.0), targets, depth_plane, weights,
+                                                     ssim_weight, noise, noise_ratio)
+    gI = np.where(I <= 1.0, gx, 0.0)
     gV = 2.0 * V * gI
-    return total, np.array(mses), np.array(ssims), gV
+    return total, mses, ssims, gV
 
 
 def quantise_depth(depth, num_planes, split_ratio=1.0):
