@@ -43,6 +43,25 @@ __device__ __forceinline__ float2 transfer(const BlasmDev& d, const PCParam& pp,
     return transfer_ji(d, pp, c, j, i, __ldg(&d.b_col[c * d.NW + i]));
 }
 
+// Plane-independent part of the transfer function at centred indices (j, i):
+// false where every plane's transfer is zero (outside the aperture, or
+// evanescent); otherwise *E = u / (1 + sqrt(1 - u)), so that plane (p, c) has
+// phase theta0 - K * E and only a band check and a sincos remain per plane.
+__device__ __forceinline__ bool transfer_excess(const BlasmDev& d, int c, int j, int i, float bcol, float* E) {
+    const int2 ap = __ldg(&d.aperture[j]);
+    const float u = __ldg(&d.a_row[c * d.NH + j]) + bcol;
+    const bool live = i >= ap.x && i < ap.y && u < 1.0f;
+    *E = live ? blasm_excess(u) : 0.0f;
+    return live;
+}
+
+// Transfer value of one plane from the hoisted excess (scale 1/(NH*NW) included).
+__device__ __forceinline__ float2 transfer_from_excess(const PCParam& pp, float E, float scale) {
+    float sn, cs;
+    sincos_reduced(pp.theta0 - pp.K * E, &sn, &cs);
+    return make_float2(cs * scale, sn * scale);
+}
+
 // amplitude clamp to 1 keeping the phase (reference: generate_complex_field(clamp(|U|,0,1), angle(U)))
 __device__ __forceinline__ float2 clamp_amplitude(float2 u) {
     const float r2 = u.x * u.x + u.y * u.y;
@@ -70,12 +89,16 @@ struct ColSplit {
     int head_npass;
     int rl;
     int mb;
+    int ntw;  // twiddle-table prefix the passes read (n / smallest radix), copied to shared memory
 };
 
 // K2 (register-spectrum variant): one column per CTA. Forward column FFT;
-// the last forward pass leaves its butterflies in registers; for each plane the
-// first inverse pass (same radix, same elements) multiplies by the transfer
-// function straight from registers. Two shared buffers per column.
+// the last forward pass leaves its butterflies in registers together with the
+// plane-independent transfer excess E of each element; for each plane the first
+// inverse pass (same radix, same elements) multiplies by that plane's transfer
+// function straight from registers, and the last inverse pass writes the kept
+// rows to global memory. Shared memory: two FFT buffers, the twiddle prefix and
+// the excess of every element (-1 where no plane propagates it).
 template <int RL, int MB>
 __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(BlasmDev d, ColSplit cs,
                                                                          const float2* __restrict__ A,
@@ -84,10 +107,13 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
     const int NH = d.NH, NW = d.NW, ld = fft_ld(NH);
     float2* b0 = sm;
     float2* b1 = sm + ld;
+    float2* tw = sm + 2 * ld;
+    float* sE = (float*)(tw + cs.ntw);
+    for (int t = threadIdx.x; t < cs.ntw; t += blockDim.x) tw[t] = __ldg(&d.col.tw[t]);
+    __syncthreads();
     const int c = blockIdx.x / NW, kx = blockIdx.x - c * NW;
     const int y0 = (NH >> 1) - (d.pH >> 1), pH = d.pH;
     const float2* src = A + (size_t)c * pH * NW + kx;
-    const float2* tw = d.col.tw;
     float2* buf = fft_run_passes(
         [=](int, int e) {
             const int y = e - y0;
@@ -95,6 +121,9 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
         },
         b0, b1, ld, 0, NH, cs.head_code, cs.head_npass, 1, tw, false);
     const int nbL = NH / RL;  // = stride Ns of the last pass; k = j, twiddle stride 1
+    int ci = kx + (NW >> 1);
+    if (ci >= NW) ci -= NW;
+    const float bcol = __ldg(&d.b_col[c * NW + ci]);
     float2 spec[MB][RL];
 #pragma unroll
     for (int b = 0; b < MB; b++) {
@@ -103,21 +132,24 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
             float2 v[RL];
 #pragma unroll
             for (int r = 0; r < RL; r++) v[r] = buf[fft_pad(j + r * nbL)];
-            apply_twiddles<RL>(v, __ldg(&tw[j]));
+            apply_twiddles<RL>(v, tw[j]);
             dft<RL>(v, false);
 #pragma unroll
-            for (int r = 0; r < RL; r++) spec[b][r] = v[r];
+            for (int r = 0; r < RL; r++) {
+                spec[b][r] = v[r];
+                int jj = j + r * nbL + (NH >> 1);
+                if (jj >= NH) jj -= NH;
+                float E;
+                sE[j + r * nbL] = transfer_excess(d, c, jj, ci, bcol, &E) ? E : -1.0f;
+            }
         }
     }
     __syncthreads();
-    int i = kx + (NW >> 1);
-    if (i >= NW) i -= NW;
-    const int row0 = (NH >> 1) - (d.out_h >> 1);
+    const int row0 = (NH >> 1) - (d.out_h >> 1), oh = d.out_h;
     for (int p = 0; p < d.P; p++) {
         const int pc = p * d.C + c;
         const PCParam pp = d.pcp[pc];
-        const bool col_ok = i >= pp.i0 && i < pp.i1;
-        const float bcol = __ldg(&d.b_col[c * NW + i]);
+        const bool col_ok = ci >= pp.i0 && ci < pp.i1;
 #pragma unroll
         for (int b = 0; b < MB; b++) {
             const int j = threadIdx.x + b * blockDim.x;
@@ -127,7 +159,9 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
                 for (int r = 0; r < RL; r++) {
                     int jj = j + r * nbL + (NH >> 1);
                     if (jj >= NH) jj -= NH;
-                    v[r] = col_ok ? cmul(spec[b][r], transfer_ji(d, pp, c, jj, i, bcol)) : make_float2(0.f, 0.f);
+                    const float E = sE[j + r * nbL];
+                    const bool on = col_ok && E >= 0.0f && jj >= pp.j0 && jj < pp.j1;
+                    v[r] = on ? cmul(spec[b][r], transfer_from_excess(pp, E, d.scale)) : make_float2(0.f, 0.f);
                 }
                 dft<RL>(v, true);
 #pragma unroll
@@ -135,17 +169,20 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
             }
         }
         __syncthreads();
-        float2* res = fft_run_passes([b0](int, int e) { return b0[fft_pad(e)]; }, b1, b0, ld, 0, NH, cs.head_code,
-                                     cs.head_npass, RL, tw, true);
-        float2* dst = B + (size_t)pc * d.out_h * NW + kx;
-        for (int y = threadIdx.x; y < d.out_h; y += blockDim.x) dst[(size_t)y * NW] = res[fft_pad(row0 + y)];
-        __syncthreads();
+        float2* dst = B + (size_t)pc * oh * NW + kx;
+        fft_run_passes_to([b0](int, int e) { return b0[fft_pad(e)]; },
+                          [=](int, int a, float2 v) {
+                              const int y = a - row0;
+                              if ((unsigned)y < (unsigned)oh) dst[(size_t)y * NW] = v;
+                          },
+                          b1, b0, ld, 0, NH, cs.head_code, cs.head_npass, RL, tw, true);
     }
 }
 
 // K2b (register variant): per plane forward column FFT whose last pass leaves
 // its butterflies in registers, multiplied by conj(transfer) and accumulated
-// there; then the first inverse pass starts from the accumulator.
+// there; then the first inverse pass starts from the accumulator and the last
+// one writes the kept rows to global memory.
 template <int RL, int MB>
 __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(BlasmDev d, ColSplit cs,
                                                                          const float2* __restrict__ Bt,
@@ -154,13 +191,22 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
     const int NH = d.NH, NW = d.NW, ld = fft_ld(NH);
     float2* b0 = sm;
     float2* b1 = sm + ld;
+    float2* tw = sm + 2 * ld;
+    float* sE = (float*)(tw + cs.ntw);
+    for (int t = threadIdx.x; t < cs.ntw; t += blockDim.x) tw[t] = __ldg(&d.col.tw[t]);
     const int c = blockIdx.x / NW, kx = blockIdx.x - c * NW;
     const int row0 = (NH >> 1) - (d.out_h >> 1), oh = d.out_h;
-    const float2* tw = d.col.tw;
     const int nbL = NH / RL;
-    int i = kx + (NW >> 1);
-    if (i >= NW) i -= NW;
-    const float bcol = __ldg(&d.b_col[c * NW + i]);
+    int ci = kx + (NW >> 1);
+    if (ci >= NW) ci -= NW;
+    const float bcol = __ldg(&d.b_col[c * NW + ci]);
+    for (int e = threadIdx.x; e < NH; e += blockDim.x) {
+        int jj = e + (NH >> 1);
+        if (jj >= NH) jj -= NH;
+        float E;
+        sE[e] = transfer_excess(d, c, jj, ci, bcol, &E) ? E : -1.0f;
+    }
+    __syncthreads();
     float2 acc[MB][RL];
 #pragma unroll
     for (int b = 0; b < MB; b++)
@@ -176,7 +222,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
             },
             b0, b1, ld, 0, NH, cs.head_code, cs.head_npass, 1, tw, false);
         const PCParam pp = d.pcp[pc];
-        const bool col_ok = i >= pp.i0 && i < pp.i1;
+        const bool col_ok = ci >= pp.i0 && ci < pp.i1;
 #pragma unroll
         for (int b = 0; b < MB; b++) {
             const int j = threadIdx.x + b * blockDim.x;
@@ -184,14 +230,16 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
                 float2 v[RL];
 #pragma unroll
                 for (int r = 0; r < RL; r++) v[r] = buf[fft_pad(j + r * nbL)];
-                apply_twiddles<RL>(v, __ldg(&tw[j]));
+                apply_twiddles<RL>(v, tw[j]);
                 dft<RL>(v, false);
                 if (col_ok) {
 #pragma unroll
                     for (int r = 0; r < RL; r++) {
                         int jj = j + r * nbL + (NH >> 1);
                         if (jj >= NH) jj -= NH;
-                        acc[b][r] = cadd(acc[b][r], cmulc(v[r], transfer_ji(d, pp, c, jj, i, bcol)));
+                        const float E = sE[j + r * nbL];
+                        if (E >= 0.0f && jj >= pp.j0 && jj < pp.j1)
+                            acc[b][r] = cadd(acc[b][r], cmulc(v[r], transfer_from_excess(pp, E, d.scale)));
                     }
                 }
             }
@@ -211,12 +259,15 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
         }
     }
     __syncthreads();
-    float2* res = fft_run_passes([b0](int, int e) { return b0[fft_pad(e)]; }, b1, b0, ld, 0, NH, cs.head_code,
-                                 cs.head_npass, RL, tw, true);
     const int in_h = d.input_mode == 0 ? d.H : d.pH;
     const int r0 = (NH >> 1) - (in_h >> 1);
     float2* dst = Ab + (size_t)c * in_h * NW + kx;
-    for (int y = threadIdx.x; y < in_h; y += blockDim.x) dst[(size_t)y * NW] = res[fft_pad(r0 + y)];
+    fft_run_passes_to([b0](int, int e) { return b0[fft_pad(e)]; },
+                      [=](int, int a, float2 v) {
+                          const int y = a - r0;
+                          if ((unsigned)y < (unsigned)in_h) dst[(size_t)y * NW] = v;
+                      },
+                      b1, b0, ld, 0, NH, cs.head_code, cs.head_npass, RL, tw, true);
 }
 
 
@@ -239,7 +290,7 @@ void launch_cols_reg_r16(bool adjoint, const BlasmDev& d, const ColSplit& cs, co
 #define CVQPG_DEFINE_COLS_REG(RL)                                                                                  \
     void launch_cols_reg_r##RL(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out, \
                                cudaStream_t s) {                                                                   \
-        const size_t sm = (size_t)2 * fft_ld(d.NH) * sizeof(float2);                                              \
+        const size_t sm = ((size_t)2 * fft_ld(d.NH) + cs.ntw) * sizeof(float2) + (size_t)d.NH * sizeof(float);                                              \
         if (!adjoint) {                                                                                            \
             if (cs.mb == 1) {                                                                                      \
                 cudaFuncSetAttribute(blasm_cols_fwd_reg_kernel<RL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, \

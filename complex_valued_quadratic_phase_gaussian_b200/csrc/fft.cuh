@@ -154,12 +154,19 @@ __device__ __forceinline__ void split_index(int j, int Ns, float inv_ns, int& q,
 // ---------------------------------------------------------------------------
 // one out-of-place Stockham pass over 2^tshift interleaved sequences. `src(t, a)`
 // returns element a of sequence t (a shared-memory read, or for the first pass a
-// global read with a pointwise operation fused into it). Each thread holds a
-// single butterfly at a time, so the register footprint is one radix.
+// global read with a pointwise operation fused into it); `sink(t, a, v)` stores
+// element a of the result (a shared-memory write, or for the last pass a global
+// write of the kept elements). Each thread holds a single butterfly at a time,
+// so the register footprint is one radix. `tw` may point to shared or global memory.
 // ---------------------------------------------------------------------------
-template <int R, typename Src>
-__device__ __forceinline__ void fft_pass(Src src, float2* __restrict__ out, int ld, int tshift, int n, int Ns,
-                                         const float2* __restrict__ tw, bool inv) {
+struct SmemSink {
+    float2* out;
+    int ld;
+    __device__ __forceinline__ void operator()(int t, int a, float2 v) const { out[t * ld + fft_pad(a)] = v; }
+};
+
+template <int R, typename Src, typename Sink>
+__device__ __forceinline__ void fft_pass(Src src, Sink sink, int tshift, int n, int Ns, const float2* tw, bool inv) {
     const int nb = n / R;
     const int total = nb << tshift;
     const int stride = n / (Ns * R);
@@ -173,62 +180,78 @@ __device__ __forceinline__ void fft_pass(Src src, float2* __restrict__ out, int 
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = src(t, j + r * nb);
         if (Ns > 1) {
-            float2 w = __ldg(&tw[k * stride]);
+            float2 w = tw[k * stride];
             if (inv) w.y = -w.y;
             apply_twiddles<R>(v, w);
         }
         dft<R>(v, inv);
         const int o = q * Ns * R + k;
-        float2* dst = out + t * ld;
 #pragma unroll
-        for (int r = 0; r < R; r++) dst[fft_pad(o + r * Ns)] = v[r];
+        for (int r = 0; r < R; r++) sink(t, o + r * Ns, v[r]);
     }
     __syncthreads();
 }
 
-template <typename Src>
-__device__ __forceinline__ void fft_pass_dispatch(int R, Src src, float2* out, int ld, int tshift, int n, int Ns,
+template <typename Src, typename Sink>
+__device__ __forceinline__ void fft_pass_dispatch(int R, Src src, Sink sink, int tshift, int n, int Ns,
                                                   const float2* tw, bool inv) {
     switch (R) {
-        case 16: fft_pass<16>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 8: fft_pass<8>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 4: fft_pass<4>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 2: fft_pass<2>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 3: fft_pass<3>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 5: fft_pass<5>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 7: fft_pass<7>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 11: fft_pass<11>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 13: fft_pass<13>(src, out, ld, tshift, n, Ns, tw, inv); break;
-        case 17: fft_pass<17>(src, out, ld, tshift, n, Ns, tw, inv); break;
+        case 16: fft_pass<16>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 8: fft_pass<8>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 4: fft_pass<4>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 2: fft_pass<2>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 3: fft_pass<3>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 5: fft_pass<5>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 7: fft_pass<7>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 11: fft_pass<11>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 13: fft_pass<13>(src, sink, tshift, n, Ns, tw, inv); break;
+        case 17: fft_pass<17>(src, sink, tshift, n, Ns, tw, inv); break;
         default: break;
     }
 }
 
 // Run `npass` passes (radices packed 5 bits each in `code`, first one in the low
-// bits) starting at stride Ns0, ping-ponging a, b; the first pass reads through
-// `first` and writes a. Returns the buffer holding the result. The caller must
-// synchronise before `first` reads shared data written earlier; ends with a barrier.
-template <typename First>
-__device__ __forceinline__ float2* fft_run_passes(First first, float2* a, float2* b, int ld, int tshift, int n,
-                                                  unsigned long long code, int npass, int Ns0, const float2* tw,
-                                                  bool inv) {
+// bits) starting at stride Ns0. The first pass reads through `first`; passes
+// ping-pong between the shared buffers a and b; the last pass stores through
+// `last` instead. The caller must synchronise before `first` reads shared data
+// written earlier; ends with a barrier.
+template <typename First, typename Last>
+__device__ __forceinline__ void fft_run_passes_to(First first, Last last, float2* a, float2* b, int ld, int tshift,
+                                                  int n, unsigned long long code, int npass, int Ns0,
+                                                  const float2* tw, bool inv) {
     int Ns = Ns0;
     int R = (int)(code & 31ull);
-    fft_pass_dispatch(R, first, a, ld, tshift, n, Ns, tw, inv);
+    if (npass == 1) {
+        fft_pass_dispatch(R, first, last, tshift, n, Ns, tw, inv);
+        return;
+    }
+    fft_pass_dispatch(R, first, SmemSink{a, ld}, tshift, n, Ns, tw, inv);
     Ns *= R;
     float2* cur = a;
     float2* nxt = b;
     for (int p = 1; p < npass; p++) {
         R = (int)((code >> (5 * p)) & 31ull);
         const float2* in = cur;
-        fft_pass_dispatch(R, [in, ld](int t, int e) { return in[t * ld + fft_pad(e)]; }, nxt, ld, tshift, n, Ns, tw,
-                          inv);
+        auto src = [in, ld](int t, int e) { return in[t * ld + fft_pad(e)]; };
+        if (p + 1 < npass)
+            fft_pass_dispatch(R, src, SmemSink{nxt, ld}, tshift, n, Ns, tw, inv);
+        else
+            fft_pass_dispatch(R, src, last, tshift, n, Ns, tw, inv);
         Ns *= R;
         float2* tmp = cur;
         cur = nxt;
         nxt = tmp;
     }
-    return cur;
+}
+
+// Same, with the result left in shared memory; returns the buffer holding it.
+template <typename First>
+__device__ __forceinline__ float2* fft_run_passes(First first, float2* a, float2* b, int ld, int tshift, int n,
+                                                  unsigned long long code, int npass, int Ns0, const float2* tw,
+                                                  bool inv) {
+    float2* res = (npass & 1) ? a : b;
+    fft_run_passes_to(first, SmemSink{res, ld}, a, b, ld, tshift, n, code, npass, Ns0, tw, inv);
+    return res;
 }
 
 // Full transform of 2^tshift sequences (all passes of the plan from stride 1).
@@ -236,6 +259,13 @@ template <typename First>
 __device__ __forceinline__ float2* fft_run(First first, float2* a, float2* b, int ld, int tshift, FftPlan plan,
                                            bool inv) {
     return fft_run_passes(first, a, b, ld, tshift, plan.n, plan.code, plan.npass, 1, plan.tw, inv);
+}
+
+// Full transform whose last pass stores through `last`.
+template <typename First, typename Last>
+__device__ __forceinline__ void fft_run_to(First first, Last last, float2* a, float2* b, int ld, int tshift,
+                                           FftPlan plan, bool inv) {
+    fft_run_passes_to(first, last, a, b, ld, tshift, plan.n, plan.code, plan.npass, 1, plan.tw, inv);
 }
 
 // Host: factor n into supported radices (16/8/4/2 first, then 3..17).
