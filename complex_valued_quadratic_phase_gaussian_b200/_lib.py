@@ -45,6 +45,7 @@ _SIGNATURES = {
     "cvqpg_loss_workspace_size": [_p, _psz],
     "cvqpg_loss_target_range": [_p, _i, _i, _i, _i, _p, _p, _sz, _p],
     "cvqpg_loss_forward_backward": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
+    "cvqpg_gemm_bf16_tn": [_p, _i, _p, _i, _i, _i, _i, _p, _i, _p, _p],
     "cvqpg_fit_workspace_size": [_p, _psz],
     "cvqpg_fit_setup": [_p, _p, _p, _sz],
     "cvqpg_fit_step": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],

@@ -2,7 +2,8 @@
 
 The library is a plain C-ABI CUDA library (no torch types cross its boundary),
 compiled from ``csrc/*.cu`` with ``-gencode arch=compute_100a,code=sm_100a``.
-It is rebuilt only when a source or header is newer than the existing ``.so``.
+It is rebuilt only when a source or header is newer than the existing ``.so``;
+an object is recompiled when its source or any shared header is newer than it.
 """
 import glob
 import os
@@ -52,13 +53,17 @@ def build(force=False, verbose=False):
     nvcc = _nvcc()
     objs = []
     procs = []
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    newest_header = max((os.path.getmtime(h) for h in headers), default=0.0)
     for src in sources():
         obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_header):
+            continue  # object is newer than its source and every shared header
         cmd = [nvcc, *NVCC_FLAGS, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
-        objs.append(obj)
     failed = []
     for src, p in procs:
         out, _ = p.communicate()

@@ -333,6 +333,42 @@ CVQPG_API int cvqpg_fit_evaluate(const cvqpg_fit_params* prm, const float* param
                                  float* field_out, float* planes_out, int32_t* status, void* workspace,
                                  size_t workspace_bytes, void* stream);
 
+/* ---- BF16 tensor-core GEMM (learned initialiser) ---------------------------
+ *
+ * No reference counterpart: the reference has no learned part. C[M,N] =
+ * A[M,K] * B[N,K]^T with A and B BF16 row-major (K contiguous), FP32
+ * accumulation in tensor memory (tcgen05, sm_100a), and a fused epilogue:
+ *   F32        out_f32[m][n] = C (split-K: slab `split` at out_f32 + split*split_stride)
+ *   BIAS       out_f32 = C + bias[n]
+ *   BIAS_GELU  Z = C + bias[n] -> out_f32 (if non-null); H = GELU(Z) (erf form) ->
+ *              out_bf16 [M][ld_bf16] and/or out_bf16_t [N][ld_t] (transposed)
+ *   DGELU      dZ = C * GELU'(zin[m][n]) -> out_bf16 and/or out_bf16_t
+ * Columns n >= valid_n are written as 0 in the BF16 outputs (padding).
+ * M and N multiples of 128, K a multiple of 64*splits, lda/ldb multiples of 8,
+ * 16-byte aligned operands; splits > 1 only with F32. status[0] (device int) is
+ * set non-zero if a pipeline wait timed out; the kernel then writes nothing. */
+#define CVQPG_GEMM_EPI_F32 0
+#define CVQPG_GEMM_EPI_BIAS 1
+#define CVQPG_GEMM_EPI_BIAS_GELU 2
+#define CVQPG_GEMM_EPI_DGELU 3
+typedef struct cvqpg_gemm_epilogue {
+    int mode;
+    int valid_n;
+    const float* bias;
+    const float* zin;
+    int ld_z;
+    int ld_f32;
+    float* out_f32;
+    long long split_stride;
+    void* out_bf16;
+    void* out_bf16_t;
+    int ld_bf16;
+    int ld_t;
+} cvqpg_gemm_epilogue;
+
+CVQPG_API int cvqpg_gemm_bf16_tn(const void* A, int lda, const void* B, int ldb, int M, int N, int K,
+                                 const cvqpg_gemm_epilogue* epilogue, int splits, int* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
