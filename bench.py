@@ -385,6 +385,10 @@ def run_ours(args, wl, dist, world, rank, local):
         cpu = {"value": v, "unit": "it/s", "cores": cores, "kind": "port", "sample": desc,
                "component_seconds": comp}
 
+    ttp = None
+    if rank == 0 and world == 1 and args.workload == "rgb1080" and not args.no_time_to_psnr:
+        ttp = run_time_to_psnr()
+
     if rank != 0:
         return None
     pH, pW = cfg.resolved_pad()
@@ -414,7 +418,30 @@ def run_ours(args, wl, dist, world, rank, local):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if ttp is not None:
+        line["time_to_psnr"] = ttp
     return line
+
+
+def run_time_to_psnr():
+    """Second half of the metric: time for the learned-init fit to reach the plain-init fit's
+    2000-iteration per-plane PSNR at 1920x1080 RGB (12 Gaussians per 16x16 tile = 97,920)."""
+    from complex_valued_quadratic_phase_gaussian_b200 import learned as L
+    t0 = time.time()
+    w, T2, info = L.train_initialiser(num_scenes=64, H=256, W=256, iters=400, steps=3000)
+    torch.cuda.synchronize()
+    train_s = time.time() - t0
+    res = L.time_to_psnr_experiment(w, T2, H=1080, W=1920, plain_iters=2000, eval_every=50)
+    res["gaussians"] = L.num_gaussians(1080, 1920)
+    res["training"] = {"wall_seconds": round(train_s, 2), "pairs": info["pairs"],
+                       "fits": "2 rounds x 64 fits of 256x256 crops with 1080p statistics, 400 iterations, "
+                               "batched fitter; round 2 starts from round 1's network",
+                       "mlp": "1024-512-512-156 GELU, BF16 tcgen05 GEMMs, FP32 Adam, 3000 steps x 8192 tiles",
+                       "final_loss": info["loss_round2"][-1][1]}
+    res["note"] = ("times are fit-iteration device time (CUDA events), evaluation excluded; 'learned' includes "
+                   "the network's prediction; 'constant' is the ablation without the network (every slot at the "
+                   "mean training target)")
+    return res
 
 
 def run_reference_cpu_arm(args, wl, rank):
@@ -475,6 +502,8 @@ def main():
     ap.add_argument("--primitive", default="curv", choices=["curv", "flat"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-time-to-psnr", action="store_true",
+                    help="skip the learned-vs-plain time-to-PSNR experiment (about a minute at N=1)")
     args = ap.parse_args()
     world, rank, local = dist_env()
     wl = WORKLOADS[args.workload]

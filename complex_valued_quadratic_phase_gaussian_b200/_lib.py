@@ -46,6 +46,12 @@ _SIGNATURES = {
     "cvqpg_loss_target_range": [_p, _i, _i, _i, _i, _p, _p, _sz, _p],
     "cvqpg_loss_forward_backward": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
     "cvqpg_gemm_bf16_tn": [_p, _i, _p, _i, _i, _i, _i, _p, _i, _p, _p],
+    "cvqpg_mlp_weights_size": [_p, _psz],
+    "cvqpg_mlp_workspace_size": [_p, _psz],
+    "cvqpg_mlp_sync_weights": [_p, _p, _p, _sz, _p],
+    "cvqpg_mlp_forward": [_p, _p, _p, _p, _p, _sz, _p, _p],
+    "cvqpg_mlp_gradients": [_p, _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p],
+    "cvqpg_mlp_train_step": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p],
     "cvqpg_fit_workspace_size": [_p, _psz],
     "cvqpg_fit_setup": [_p, _p, _p, _sz],
     "cvqpg_fit_step": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],

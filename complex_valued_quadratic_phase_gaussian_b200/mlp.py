@@ -64,3 +64,86 @@ def gemm_bf16_tn(A, B, mode=EPI_F32, out_f32=None, bias=None, zin=None, out_bf16
                                       int(splits), _lib.ptr(status), _lib.stream_of(A.device)),
                "cvqpg_gemm_bf16_tn")
     return status
+
+
+class MlpParams(ctypes.Structure):
+    """``cvqpg_mlp_params`` (include/cvqpg.h)."""
+    _fields_ = [("batch", ctypes.c_int), ("in_dim", ctypes.c_int), ("hidden", ctypes.c_int), ("out_dim", ctypes.c_int),
+                ("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("weight_decay", ctypes.c_float), ("reserved", ctypes.c_int)]
+
+
+class TileMLP:
+    """in_dim -> hidden -> hidden -> out_dim MLP with GELU, trained with Adam on the GPU.
+
+    ``weights`` is the flat FP32 vector of cvqpg.h (W1 | b1 | W2 | b2 | W3 | b3,
+    W3/b3 padded to a multiple of 128 rows). One instance serves one batch size.
+    """
+
+    def __init__(self, batch, in_dim=1024, hidden=512, out_dim=156, lr=3e-4, betas=(0.9, 0.999), eps=1e-8,
+                 weight_decay=0.0, weights=None, device="cuda"):
+        self.device = torch.device(device)
+        self.prm = MlpParams(int(batch), int(in_dim), int(hidden), int(out_dim), float(lr), float(betas[0]),
+                             float(betas[1]), float(eps), float(weight_decay), 0)
+        lib = _lib.lib()
+        n = _lib.size_query(lib.cvqpg_mlp_weights_size, ctypes.byref(self.prm))
+        self.ws = _lib.workspace(_lib.size_query(lib.cvqpg_mlp_workspace_size, ctypes.byref(self.prm)), self.device)
+        if weights is None:
+            from_numpy = _default_init(in_dim, hidden, out_dim)
+            weights = torch.from_numpy(from_numpy)
+        self.weights = torch.as_tensor(weights, dtype=torch.float32).to(self.device).contiguous()
+        if self.weights.numel() != n:
+            raise ValueError(f"weights must have {n} floats")
+        self.adam = torch.zeros(2 * n, dtype=torch.float32, device=self.device)
+        self.step_count = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        self.sync()
+
+    def sync(self):
+        """Refresh the BF16 weight copies after writing ``weights`` from outside."""
+        lib = _lib.lib()
+        _lib.check(lib.cvqpg_mlp_sync_weights(ctypes.byref(self.prm), _lib.ptr(self.weights), _lib.ptr(self.ws),
+                                              self.ws.numel(), _lib.stream_of(self.device)), "cvqpg_mlp_sync_weights")
+
+    def forward(self, X, out=None):
+        X = X.contiguous().float()
+        if out is None:
+            out = torch.empty((self.prm.batch, self.prm.out_dim), dtype=torch.float32, device=self.device)
+        lib = _lib.lib()
+        _lib.check(lib.cvqpg_mlp_forward(ctypes.byref(self.prm), _lib.ptr(self.weights), _lib.ptr(X), _lib.ptr(out),
+                                         _lib.ptr(self.ws), self.ws.numel(), _lib.ptr(self.status),
+                                         _lib.stream_of(self.device)), "cvqpg_mlp_forward")
+        return out
+
+    def gradients(self, X, T, out_weight):
+        grads = torch.empty_like(self.weights)
+        lib = _lib.lib()
+        _lib.check(lib.cvqpg_mlp_gradients(ctypes.byref(self.prm), _lib.ptr(self.weights), _lib.ptr(X.contiguous()),
+                                           _lib.ptr(T.contiguous()), _lib.ptr(out_weight.contiguous()),
+                                           _lib.ptr(grads), _lib.ptr(self.loss), _lib.ptr(self.ws), self.ws.numel(),
+                                           _lib.ptr(self.status), _lib.stream_of(self.device)), "cvqpg_mlp_gradients")
+        return self.loss, grads
+
+    def train_step(self, X, T, out_weight):
+        """One Adam step on (X, T); returns the device loss tensor (no host sync)."""
+        lib = _lib.lib()
+        _lib.check(lib.cvqpg_mlp_train_step(ctypes.byref(self.prm), _lib.ptr(self.weights), _lib.ptr(self.adam),
+                                            _lib.ptr(self.step_count), _lib.ptr(X), _lib.ptr(T), _lib.ptr(out_weight),
+                                            _lib.ptr(self.loss), _lib.ptr(self.ws), self.ws.numel(),
+                                            _lib.ptr(self.status), _lib.stream_of(self.device)),
+                   "cvqpg_mlp_train_step")
+        return self.loss
+
+
+def _default_init(in_dim, hidden, out_dim, seed=0):
+    """He-normal hidden layers, a small output layer, zero biases (float32, flat layout)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    op = (out_dim + 127) // 128 * 128
+    w1 = rng.normal(0, np.sqrt(2.0 / in_dim), (hidden, in_dim))
+    w2 = rng.normal(0, np.sqrt(2.0 / hidden), (hidden, hidden))
+    w3 = np.zeros((op, hidden))
+    w3[:out_dim] = rng.normal(0, 0.1 / np.sqrt(hidden), (out_dim, hidden))
+    return np.concatenate([w1.ravel(), np.zeros(hidden), w2.ravel(), np.zeros(hidden), w3.ravel(),
+                           np.zeros(op)]).astype(np.float32)

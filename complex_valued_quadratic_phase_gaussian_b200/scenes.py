@@ -55,11 +55,15 @@ def grayscale_blobs(H, W, seed=0, num_blobs=64):
     return img[None].astype(np.float32), depth.astype(np.float32)
 
 
-def rgb_blobs(H, W, seed=0, num_blobs=2000):
-    """1080p-style RGB target (coloured anisotropic blobs + 1/f noise) and a smooth 1/f depth."""
+def rgb_blobs(H, W, seed=0, num_blobs=2000, scale=None):
+    """1080p-style RGB target (coloured anisotropic blobs + 1/f noise) and a smooth 1/f depth.
+
+    ``scale`` sets the blob size unit in pixels (default min(H, W)); a crop with
+    the statistics of a 1080p scene uses scale=1080 and num_blobs scaled by area.
+    """
     rng = np.random.default_rng(seed)
     img = np.zeros((3, H, W))
-    scale = min(H, W)
+    scale = min(H, W) if scale is None else scale
     for _ in range(num_blobs):
         cx, cy = rng.uniform(0, W), rng.uniform(0, H)
         sx, sy = rng.uniform(0.004, 0.03, 2) * scale
@@ -82,6 +86,12 @@ def rgb_blobs(H, W, seed=0, num_blobs=2000):
     img /= max(img.max(), 1e-12)
     depth = _fbm(rng, H, W, 2.0)
     return img.astype(np.float32), depth.astype(np.float32)
+
+
+def rgb_crop_like_1080p(H, W, seed=0):
+    """An H x W scene with the per-pixel statistics of ``rgb_blobs(1080, 1920)`` (blob sizes and density)."""
+    n = max(1, int(round(2000 * H * W / (1080.0 * 1920.0))))
+    return rgb_blobs(H, W, seed=seed, num_blobs=n, scale=1080)
 
 
 def _gaussian_kernel_2d(length, sigma):

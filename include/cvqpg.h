@@ -369,6 +369,46 @@ typedef struct cvqpg_gemm_epilogue {
 CVQPG_API int cvqpg_gemm_bf16_tn(const void* A, int lda, const void* B, int ldb, int M, int N, int K,
                                  const cvqpg_gemm_epilogue* epilogue, int splits, int* status, void* stream);
 
+/* ---- per-tile MLP of the learned initialiser --------------------------------
+ *
+ * No reference counterpart: the reference starts every fit from random
+ * Gaussians. in_dim -> hidden -> hidden -> out_dim with GELU after the hidden
+ * layers; GEMMs on the tensor cores (cvqpg_gemm_bf16_tn, BF16 operands, FP32
+ * accumulation); FP32 master weights and Adam. in_dim and hidden must be
+ * multiples of 128. Weights are one FP32 vector (cvqpg_mlp_weights_size floats):
+ *   W1 [hidden][in_dim] | b1 [hidden] | W2 [hidden][hidden] | b2 [hidden] |
+ *   W3 [out_pad][hidden] | b3 [out_pad],  out_pad = out_dim rounded up to 128
+ * (rows >= out_dim of W3 and b3 are kept at zero). The workspace holds the
+ * activations and the BF16 weight copies; call cvqpg_mlp_sync_weights after
+ * writing the FP32 weights from outside (cvqpg_mlp_train_step keeps them in step).
+ * Loss: sum over rows m < batch and outputs j < out_dim of
+ * out_weight[j] * (Y[m][j] - T[m][j])^2, divided by batch. */
+typedef struct cvqpg_mlp_params {
+    int batch;
+    int in_dim;
+    int hidden;
+    int out_dim;
+    float lr, beta1, beta2, eps, weight_decay;
+    int reserved;
+} cvqpg_mlp_params;
+
+CVQPG_API int cvqpg_mlp_weights_size(const cvqpg_mlp_params* prm, size_t* floats);
+CVQPG_API int cvqpg_mlp_workspace_size(const cvqpg_mlp_params* prm, size_t* bytes);
+CVQPG_API int cvqpg_mlp_sync_weights(const cvqpg_mlp_params* prm, const float* weights, void* workspace,
+                                     size_t workspace_bytes, void* stream);
+/* Y [batch][out_dim] (may be null: the output then stays in the workspace). */
+CVQPG_API int cvqpg_mlp_forward(const cvqpg_mlp_params* prm, const float* weights, const float* X, float* Y,
+                                void* workspace, size_t workspace_bytes, int* status, void* stream);
+/* Forward, loss and dL/dweights (same layout as the weights), no update. */
+CVQPG_API int cvqpg_mlp_gradients(const cvqpg_mlp_params* prm, const float* weights, const float* X, const float* T,
+                                  const float* out_weight, float* grads, float* loss, void* workspace,
+                                  size_t workspace_bytes, int* status, void* stream);
+/* One Adam step (state = 2 x weights: first and second moments; step = device int,
+ * incremented; bias correction uses step + 1). Graph-capturable. */
+CVQPG_API int cvqpg_mlp_train_step(const cvqpg_mlp_params* prm, float* weights, float* adam_state, int* step,
+                                   const float* X, const float* T, const float* out_weight, float* loss,
+                                   void* workspace, size_t workspace_bytes, int* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
