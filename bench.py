@@ -214,7 +214,7 @@ def fit_config(wl, seed, primitive="curv"):
     from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig
     return FitConfig(img_size=(wl["W"], wl["H"]), num_gaussians=wl["N"], wavelengths=list(wl["wl"]),
                      pixel_pitch=wl["pitch"], num_planes=wl["P"], d_val=wl["d_val"], volume_depth=wl["vd"],
-                     primitive=primitive, warmup_iters=400, num_itrs=2000, seed=seed)
+                     primitive=primitive, warmup_iters=400, num_itrs=2000, seed=seed, autotune=True)
 
 
 def stage_bytes(cfg):
@@ -400,7 +400,7 @@ def run_ours(args, wl, dist, world, rank, local):
         "config": {"workload": f"{args.workload}_fit", "image": f"{cfg.W}x{cfg.H}", "channels": len(cfg.wavelengths),
                    "gaussians": cfg.num_gaussians, "planes": cfg.num_planes, "pad": f"{pH}x{pW}",
                    "fft_grid": f"{2 * pH}x{2 * pW}", "primitive": args.primitive, "cull": "cuda16_5sigma",
-                   "graph": True, "parallelism": f"replicas x{world}",
+                   "graph": True, "parallelism": f"replicas x{world}", "fft_plan_hint": fitter.plan_hint,
                    "l2": "inputs larger than L2 (per-iteration working set ~GBs)"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,

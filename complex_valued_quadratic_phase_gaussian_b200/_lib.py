@@ -72,11 +72,13 @@ def lib():
     """Load libcvqpg.so once; raise if it has not been built."""
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
+        # CVQPG_LIBRARY names another build of the same library (side-by-side timing of two builds)
+        path = os.environ.get("CVQPG_LIBRARY", LIB_PATH)
+        if not os.path.exists(path):
             raise RuntimeError(
-                f"{LIB_PATH} is missing: build it with "
+                f"{path} is missing: build it with "
                 "`python -m complex_valued_quadratic_phase_gaussian_b200.build` (needs nvcc)")
-        handle = ctypes.CDLL(LIB_PATH)
+        handle = ctypes.CDLL(path)
         for name, argtypes in _SIGNATURES.items():
             fn = getattr(handle, name)
             fn.argtypes = argtypes

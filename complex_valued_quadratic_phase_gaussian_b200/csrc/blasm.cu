@@ -28,7 +28,7 @@ namespace cvqpg {
 // ---------------------------------------------------------------------------
 // host: FFT plans
 // ---------------------------------------------------------------------------
-bool make_fft_plan(int n, FftPlan* plan) {
+bool make_fft_plan(int n, FftPlan* plan, int order) {
     plan->n = n;
     plan->npass = 0;
     plan->code = 0;
@@ -40,18 +40,34 @@ bool make_fft_plan(int n, FftPlan* plan) {
         plan->npass++;
         return true;
     };
-    while (m % 16 == 0)
-        if (!push(16)) return false; else m /= 16;
-    if (m % 8 == 0) { if (!push(8)) return false; m /= 8; }
-    if (m % 4 == 0) { if (!push(4)) return false; m /= 4; }
-    if (m % 2 == 0) { if (!push(2)) return false; m /= 2; }
     const int odd[] = {3, 5, 7, 11, 13, 17};
-    for (int r : odd)
-        while (m % r == 0) {
-            if (!push(r)) return false;
-            m /= r;
-        }
-    return m == 1;
+    const int odd_desc[] = {17, 13, 11, 7, 5, 3};
+    auto push_odd = [&](const int* list) {
+        for (int k = 0; k < 6; k++)
+            while (m % list[k] == 0) {
+                if (!push(list[k])) return false;
+                m /= list[k];
+            }
+        return true;
+    };
+    auto push_pow2 = [&](bool use16) {
+        if (use16)
+            while (m % 16 == 0)
+                if (!push(16)) return false; else m /= 16;
+        while (m % 8 == 0)
+            if (!push(8)) return false; else m /= 8;
+        if (m % 4 == 0) { if (!push(4)) return false; m /= 4; }
+        if (m % 2 == 0) { if (!push(2)) return false; m /= 2; }
+        return true;
+    };
+    bool ok = true;
+    switch (order) {
+        case 1: ok = push_odd(odd_desc) && push_pow2(true); break;
+        case 2: ok = push_pow2(false) && push_odd(odd); break;
+        case 3: ok = push_odd(odd_desc) && push_pow2(false); break;
+        default: ok = push_pow2(true) && push_odd(odd); break;
+    }
+    return ok && m == 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -63,7 +79,7 @@ bool make_fft_plan(int n, FftPlan* plan) {
 // ---------------------------------------------------------------------------
 // K1: one padded row per CTA. The first FFT pass reads the splat field directly
 // (replicate guard band, Tukey window, amplitude clamp on the fly).
-__global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_kernel(BlasmDev d, const float2* __restrict__ in,
+__global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_kernel(BlasmDev d, const float2* __restrict__ in,
                                                                      float2* __restrict__ A) {
     extern __shared__ float2 sm[];
     const int ld = fft_ld(d.NW);
@@ -134,7 +150,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_kernel(BlasmDev
 
 // K3: inverse FFT of a kept row (first pass reads global), keep out_w columns
 // -> V [P*C][out_h][out_w] and optionally pred = clamp(|V|^2, 0, 1)
-__global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_kernel(BlasmDev d, const float2* __restrict__ B,
+__global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_kernel(BlasmDev d, const float2* __restrict__ B,
                                                                      float2* __restrict__ V,
                                                                      float* __restrict__ pred) {
     extern __shared__ float2 sm[];
@@ -161,7 +177,7 @@ __global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_kernel(BlasmDev d,
 // adjoint kernels (same layouts: Bt [P*C][out_h][NW], Ab [C][in_h][NW])
 // ---------------------------------------------------------------------------
 // K3b: gradient row embedded at the out_w centred columns -> forward FFT
-__global__ void __launch_bounds__(kRowThreads) blasm_rows_fwd_adj_kernel(BlasmDev d, const float2* __restrict__ gV,
+__global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_adj_kernel(BlasmDev d, const float2* __restrict__ gV,
                                                                          const float* __restrict__ gpred,
                                                                          const float2* __restrict__ Vf,
                                                                          float2* __restrict__ Bt) {
@@ -242,7 +258,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_kernel(BlasmDev
 
 // K1b: inverse row FFT (first pass reads global), keep the input columns,
 // apply the amplitude-clamp adjoint against the splat field
-__global__ void __launch_bounds__(kRowThreads) blasm_rows_inv_adj_kernel(BlasmDev d, const float2* __restrict__ Ab,
+__global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_adj_kernel(BlasmDev d, const float2* __restrict__ Ab,
                                                                          const float2* __restrict__ field,
                                                                          float2* __restrict__ gin) {
     extern __shared__ float2 sm[];
@@ -360,8 +376,10 @@ int blasm_make_dev(const cvqpg_blasm_params* p, const void* tables, size_t table
     d->G = 1;
     if ((size_t)3 * fft_ld(d->NH) * sizeof(float2) > 227 * 1024) return CVQPG_ERR_UNSUPPORTED;
     d->scale = (float)(1.0 / ((double)d->NH * (double)d->NW));
-    make_fft_plan(d->NW, &d->row);
-    make_fft_plan(d->NH, &d->col);
+    const int hint = p->plan_hint;
+    d->col_radix = hint & 31;
+    if (!make_fft_plan(d->NW, &d->row, (hint >> 8) & 7) || !make_fft_plan(d->NH, &d->col, (hint >> 5) & 7))
+        return CVQPG_ERR_UNSUPPORTED;
     const char* base = (const char*)tables;
     d->row.tw = (const float2*)(base + L.tw_row);
     d->col.tw = (const float2*)(base + L.tw_col);
@@ -396,7 +414,7 @@ constexpr size_t kSmemMax = 227 * 1024;
 // Pick the radix whose butterflies stay in registers between the column FFTs:
 // the supported radix of the plan with the smallest register footprint
 // (butterflies per thread x radix). Returns false when no variant applies.
-static bool column_split(const FftPlan& plan, ColSplit* cs) {
+static bool column_split(const FftPlan& plan, ColSplit* cs, int radix_hint) {
     static const int kRL[] = {3, 5, 7, 8, 11, 13, 16};
     int best = -1, best_mb = 0, best_score = 1 << 30;
     for (int p = 0; p < plan.npass; p++) {
@@ -408,7 +426,8 @@ static bool column_split(const FftPlan& plan, ColSplit* cs) {
         const int mb = (nb + kColThreads - 1) / kColThreads;
         const int mbr = mb <= 1 ? 1 : (mb <= 2 ? 2 : 0);
         if (!mbr) continue;
-        const int score = mbr * r;
+        // the hinted radix wins when the plan has it; otherwise the smallest register footprint
+        const int score = (radix_hint && r == radix_hint) ? -1 : mbr * r;
         if (score < best_score) {
             best_score = score;
             best = p;
@@ -436,7 +455,7 @@ static bool column_split(const FftPlan& plan, ColSplit* cs) {
 
 static void launch_columns(bool adjoint, const BlasmDev& d, const float2* in, float2* out, cudaStream_t s) {
     ColSplit cs;
-    if (column_split(d.col, &cs)) {
+    if (column_split(d.col, &cs, d.col_radix)) {
         switch (cs.rl) {
             case 3: launch_cols_reg_r3(adjoint, d, cs, in, out, s); return;
             case 5: launch_cols_reg_r5(adjoint, d, cs, in, out, s); return;

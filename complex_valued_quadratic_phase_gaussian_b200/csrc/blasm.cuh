@@ -28,6 +28,7 @@ struct BlasmDev {
     int out_h, out_w;  // output crop (H, W in the fit; pH, pW for the full reconstruction)
     int input_mode;    // 0: splat field [C,H,W] (+pad, window, amplitude clamp); 1: padded field [C,pH,pW]
     int G;             // columns per column-pass CTA (tiled layout width)
+    int col_radix;     // radix the column kernels keep in registers (0 = automatic)
     float scale;       // 1 / (NH * NW)
     FftPlan row, col;  // NW and NH plans
     const float* wy;   // Tukey window [pH]

@@ -268,8 +268,10 @@ __device__ __forceinline__ void fft_run_to(First first, Last last, float2* a, fl
     fft_run_passes_to(first, last, a, b, ld, tshift, plan.n, plan.code, plan.npass, 1, plan.tw, inv);
 }
 
-// Host: factor n into supported radices (16/8/4/2 first, then 3..17).
-// Returns false when n has a prime factor above 17.
-bool make_fft_plan(int n, FftPlan* plan);
+// Host: factor n into supported radices in one of four orders (0: 16/8/4/2
+// first, then 3..17; 1: odd radices first, largest first, then 16/8/4/2;
+// 2: 8/4/2 only, then odd; 3: odd first, then 8/4/2). Returns false when n has
+// a prime factor above 17 or needs more than kMaxPasses passes.
+bool make_fft_plan(int n, FftPlan* plan, int order = 0);
 
 }  // namespace cvqpg

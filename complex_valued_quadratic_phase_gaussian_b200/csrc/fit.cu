@@ -54,6 +54,7 @@ static int fit_dims(const cvqpg_fit_params* q, cvqpg_blasm_params* bp, cvqpg_los
     for (int i = 0; i < 3; i++) bp->wavelengths[i] = q->wavelengths[i];
     for (int i = 0; i < 8; i++) bp->distances[i] = q->distances[i];
     bp->aperture_radius = q->aperture_radius;
+    bp->plan_hint = q->plan_hint;
     std::memset(lp, 0, sizeof(*lp));
     lp->channels = q->channels;
     lp->planes = q->planes;

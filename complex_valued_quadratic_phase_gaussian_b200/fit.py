@@ -45,7 +45,7 @@ class FitParams(ctypes.Structure):
                 ("curv_const", ctypes.c_double), ("lr", ctypes.c_double * 6), ("betas", ctypes.c_double * 3),
                 ("eps", ctypes.c_double), ("weight_decay", ctypes.c_double), ("max_grad_norm", ctypes.c_double),
                 ("loss_weights", ctypes.c_float * 3), ("ssim_weight", ctypes.c_float),
-                ("noise_ratio", ctypes.c_float), ("reserved", ctypes.c_float), ("seed", ctypes.c_ulonglong)]
+                ("noise_ratio", ctypes.c_float), ("plan_hint", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
 
 
 @dataclass
@@ -74,6 +74,8 @@ class FitConfig:
     pair_capacity: Optional[int] = None
     inject_noise: bool = True
     history_len: int = 4096
+    plan_hint: int = 0                       # FFT plan of the propagation (autotune.py); 0 = defaults
+    autotune: bool = False                   # pick plan_hint by measurement (cached per grid)
 
     @property
     def W(self):
@@ -207,6 +209,11 @@ class Fitter:
         p.ssim_weight = 0.025 * 0.2
         p.noise_ratio = 1e-3
         p.seed = int(cfg.seed)
+        p.plan_hint = int(cfg.plan_hint)
+        if cfg.autotune:
+            from .autotune import tune_for
+            p.plan_hint = int(tune_for(cfg, device=device)[0])
+        self.plan_hint = p.plan_hint
         self.params = p
         lib = _lib.lib()
         self._lib = lib

@@ -132,7 +132,8 @@ def decode(Y, H, W):
 def scene_config(H, W, iters, seed=0, **kw):
     """FitConfig of the headline RGB setting (639/515/473 nm, 3.74 um, 3 planes) at H x W, 12 Gaussians per tile."""
     base = dict(img_size=(W, H), num_gaussians=num_gaussians(H, W), wavelengths=[639e-9, 515e-9, 473e-9],
-                pixel_pitch=3.74e-6, num_planes=3, d_val=1e-3, volume_depth=1e-3, num_itrs=iters, seed=seed)
+                pixel_pitch=3.74e-6, num_planes=3, d_val=1e-3, volume_depth=1e-3, num_itrs=iters, seed=seed,
+                autotune=True)
     base.update(kw)
     return FitConfig(**base)
 

@@ -26,7 +26,7 @@ class BlasmParams(ctypes.Structure):
     _fields_ = [("channels", ctypes.c_int), ("planes", ctypes.c_int), ("height", ctypes.c_int),
                 ("width", ctypes.c_int), ("pad_height", ctypes.c_int), ("pad_width", ctypes.c_int),
                 ("out_height", ctypes.c_int), ("out_width", ctypes.c_int), ("input_mode", ctypes.c_int),
-                ("reserved", ctypes.c_int), ("pixel_pitch", ctypes.c_double),
+                ("plan_hint", ctypes.c_int), ("pixel_pitch", ctypes.c_double),
                 ("wavelengths", ctypes.c_double * 3), ("distances", ctypes.c_double * 8),
                 ("aperture_radius", ctypes.c_double)]
 
@@ -50,7 +50,7 @@ class BlasmPlan:
     """Device tables + workspace for one propagation geometry."""
 
     def __init__(self, channels, height, width, pad_size, wavelengths, distances, pixel_pitch,
-                 aperture_radius=None, out_size=None, input_mode=0, device="cuda"):
+                 aperture_radius=None, out_size=None, input_mode=0, device="cuda", plan_hint=0):
         if len(distances) > 8:
             raise ValueError("at most 8 planes are supported")
         self.device = torch.device(device)
@@ -67,6 +67,7 @@ class BlasmPlan:
         for i, z in enumerate(distances):
             p.distances[i] = float(z)
         p.aperture_radius = float(aperture_radius) if aperture_radius else 0.0
+        p.plan_hint = int(plan_hint)
         self.params = p
         lib = _lib.lib()
         pp = ctypes.byref(p)

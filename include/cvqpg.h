@@ -183,6 +183,15 @@ CVQPG_API int cvqpg_render_backward_cull(const float* grad_field, const float* m
  * Requirements: even H, W, pH, pW with pH >= H, pW >= W; 2pH and 2pW products
  * of primes <= 17; planes <= 8; channels 1 or 3.
  */
+/* plan_hint: which FFT plan the propagation uses (the autotuner's knob; no
+ * reference counterpart, cuFFT picks its own plans). 0 everywhere = defaults.
+ *   bits [0,5)  radix kept in registers by the column kernels (0 = automatic);
+ *   bits [5,8)  radix order of the column FFTs, bits [8,11) of the row FFTs:
+ *               0 radix 16 first then 8/4/2 then odd, 1 odd first then 16/8/4/2,
+ *               2 radix 8 first then 4/2 then odd, 3 odd first then 8/4/2. */
+#define CVQPG_PLAN_HINT(col_radix, col_order, row_order) \
+    ((col_radix) | ((col_order) << 5) | ((row_order) << 8))
+
 typedef struct cvqpg_blasm_params {
     int channels;
     int planes;
@@ -190,7 +199,7 @@ typedef struct cvqpg_blasm_params {
     int pad_height, pad_width;  /* pH, pW (the reference pad_size)             */
     int out_height, out_width;  /* output crop; 0 = (H, W)                     */
     int input_mode;             /* 0 or 1, see above                           */
-    int reserved;
+    int plan_hint;              /* FFT plan choice, 0 = default (CVQPG_PLAN_*)  */
     double pixel_pitch;         /* metres                                      */
     double wavelengths[3];      /* metres, one per channel                     */
     double distances[8];        /* metres, one per plane                       */
@@ -303,7 +312,7 @@ typedef struct cvqpg_fit_params {
     float loss_weights[3];  /* [1, 1, 1] */
     float ssim_weight;      /* 0.005 */
     float noise_ratio;      /* 1e-3 */
-    float reserved;
+    int plan_hint;          /* FFT plan choice of the propagation, 0 = default (CVQPG_PLAN_*) */
     unsigned long long seed;
 } cvqpg_fit_params;
 

@@ -50,3 +50,14 @@ def test_shard_balances_cost_and_covers_every_job():
     assert sorted(j.tag for p in parts for j in p) == list(range(len(jobs)))
     loads = [sum(j.cost() for j in p) for p in parts]
     assert max(loads) == cfgs[3].W * cfgs[3].H * 500  # the largest job alone bounds the makespan
+
+
+def test_autotune_plans_factor_every_grid_of_the_configs():
+    from complex_valued_quadratic_phase_gaussian_b200.autotune import candidates, plan_radices
+    for n in (1152, 2816, 4480, 1664, 2176, 2688, 352, 480):
+        for order in range(4):
+            r = plan_radices(n, order)
+            assert r is not None and int(np.prod(r)) == n
+        assert len(set(tuple(plan_radices(n, o)) for o in range(4))) >= 2
+    hs = candidates(2816, 4480)
+    assert 11 in hs and len(hs) == len(set(hs))  # 11 = the default plan with its automatic register radix
