@@ -40,7 +40,8 @@ struct FitLayout {
 static int fit_dims(const cvqpg_fit_params* q, cvqpg_blasm_params* bp, cvqpg_loss_params* lp) {
     if (!q) return CVQPG_ERR_ARG;
     if (q->channels != 1 && q->channels != 3) return CVQPG_ERR_CHANNELS;
-    if (q->num_gaussians < 0 || q->pair_capacity < 0 || q->cull_mode < 0 || q->cull_mode > 2) return CVQPG_ERR_ARG;
+    const int cull = q->cull_mode & ~CVQPG_PHASE_ISO;
+    if (q->num_gaussians < 0 || q->pair_capacity < 0 || cull < 0 || cull > 2) return CVQPG_ERR_ARG;
     if (q->curv_mode < 0 || q->curv_mode > 2 || q->history_len < 1) return CVQPG_ERR_ARG;
     std::memset(bp, 0, sizeof(*bp));
     bp->channels = q->channels;
@@ -81,7 +82,7 @@ static int fit_layout(const cvqpg_fit_params* q, void* base, size_t cap, FitLayo
     st = loss_make_dev(&lp, ld);
     if (st != CVQPG_OK) return st;
     const int N = q->num_gaussians, C = q->channels, P = q->planes, H = q->height, W = q->width;
-    const BinRule rule = make_bin_rule(q->cull_mode, W, H, nullptr, nullptr);
+    const BinRule rule = make_bin_rule(q->cull_mode & ~CVQPG_PHASE_ISO, W, H, nullptr, nullptr);
     Carver cv(base, cap);
     L->blasm_tables = cv.take<char>(tbytes);
     L->blasm_tables_bytes = tbytes;
@@ -177,14 +178,15 @@ static void run_forward(const cvqpg_fit_params* q, const FitLayout& L, const Bla
                         StageMarks* marks = nullptr) {
     const int C = q->channels;
     const PreDev P = make_pre(q);
-    const BinRule rule = make_bin_rule(q->cull_mode, q->width, q->height, L.radii, L.radius3);
+    const BinRule rule = make_bin_rule(q->cull_mode & ~CVQPG_PHASE_ISO, q->width, q->height, L.radii, L.radius3);
     if (marks) marks->mark(s);
     launch_preprocess_forward(C, P, raw, L.records, L.radii, L.radius3, L.bin.tiles_touched, rule, s);
     if (marks) marks->mark(s);
     launch_binning(rule, L.records, L.bin, L.point_list, L.ranges, L.pair_count, s);
     if (marks) marks->mark(s);
     const float dxy2 = (float)(q->pixel_pitch * q->pixel_pitch);
-    launch_splat_forward(C, rule, L.ranges, L.point_list, L.records, L.kvec, dxy2, L.field, s);
+    launch_splat_forward(C, rule, L.ranges, L.point_list, L.records, L.kvec, dxy2, L.field, s,
+                         (q->cull_mode & CVQPG_PHASE_ISO) != 0);
     if (marks) marks->mark(s);
     blasm_forward(bd, L.field, L.vfield, L.pred, L.blasm_ws, s, marks);
     launch_loss(ld, L.pred, targets, depth_plane, target_range, iteration, L.gpred, L.loss_partials, L.loss_out, s);
@@ -262,9 +264,10 @@ static int fit_step_impl(const cvqpg_fit_params* q, float* params, float* grads,
     float* sg = L.splat_grads;
     SplatGrads out{sg, sg + 2 * N, sg + 5 * N, sg + (5 + C) * N, sg + (5 + 2 * C) * N, sg + (6 + 2 * C) * N,
                    sg + (7 + 2 * C) * N};
-    const BinRule rule = make_bin_rule(q->cull_mode, q->width, q->height, L.radii, L.radius3);
+    const BinRule rule = make_bin_rule(q->cull_mode & ~CVQPG_PHASE_ISO, q->width, q->height, L.radii, L.radius3);
     const float dxy2 = (float)(q->pixel_pitch * q->pixel_pitch);
-    launch_splat_backward(C, rule, L.ranges, L.point_list, L.records, L.kvec, dxy2, L.gfield, out, s);
+    launch_splat_backward(C, rule, L.ranges, L.point_list, L.records, L.kvec, dxy2, L.gfield, out, s,
+                          (q->cull_mode & CVQPG_PHASE_ISO) != 0);
     if (marks) marks->mark(s);
     // preprocessing adjoint + nan_to_num + norm partials
     SplatGradsIn gin{out.d_means, out.d_inv, out.d_col, out.d_ph, out.d_op, out.d_cv, out.d_ar};

@@ -412,7 +412,7 @@ __device__ __forceinline__ int list_of_tile(const BinRule& R, int tx, int ty) {
 // splat forward: one CTA per 16x16 tile, one pixel per thread, each warp an
 // 8x4 pixel block; Gaussian batches of 256 records staged in shared memory.
 // ---------------------------------------------------------------------------
-template <int C>
+template <int C, bool ISO>
 __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
     BinRule rule, const int32_t* __restrict__ ranges, const int32_t* __restrict__ point_list,
     const float4* __restrict__ rec, const float* __restrict__ k, float dxy2, float2* __restrict__ out, int W, int H,
@@ -451,7 +451,8 @@ __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
             if (!__any_sync(0xffffffffu, mahal < kMahalCut)) continue;
             const float power = fmaxf(-0.5f * mahal, -50.0f);
             const float alpha = r1.y * __expf(power);
-            const float base = 0.5f * r1.z * mahal * r1.w * dxy2;
+            // Mahalanobis QPF (c m area) or, with ISO, the isotropic form (c |r - mu|^2)
+            const float base = ISO ? 0.5f * r1.z * (dx * dx + dy * dy) * dxy2 : 0.5f * r1.z * mahal * r1.w * dxy2;
             const float4 r2 = s_rec[j][2];
             float col[C], ph[C];
             if (C == 1) {
@@ -484,16 +485,27 @@ __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
 }
 
 void launch_splat_forward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
-                          const float* records, const float* k, float dxy2, float2* out, cudaStream_t stream) {
+                          const float* records, const float* k, float dxy2, float2* out, cudaStream_t stream,
+                          bool iso) {
     const int width = rule.width, height = rule.height;
     const int gx = (width + kTile - 1) / kTile, gy = (height + kTile - 1) / kTile;
     const float4* rec = reinterpret_cast<const float4*>(records);
-    if (channels == 1)
-        splat_forward_kernel<1><<<gx * gy, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2, out,
-                                                                     width, height, gx);
-    else
-        splat_forward_kernel<3><<<gx * gy, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2, out,
-                                                                     width, height, gx);
+    const dim3 grid(gx * gy);
+    if (channels == 1) {
+        if (iso)
+            splat_forward_kernel<1, true><<<grid, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
+                                                                            out, width, height, gx);
+        else
+            splat_forward_kernel<1, false><<<grid, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
+                                                                             out, width, height, gx);
+    } else {
+        if (iso)
+            splat_forward_kernel<3, true><<<grid, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
+                                                                            out, width, height, gx);
+        else
+            splat_forward_kernel<3, false><<<grid, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
+                                                                             out, width, height, gx);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -507,7 +519,7 @@ void launch_splat_forward(int channels, const BinRule& rule, const int32_t* rang
 // ---------------------------------------------------------------------------
 constexpr int kBwdThreads = 64;
 
-template <int C>
+template <int C, bool ISO>
 __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     BinRule rule, const int32_t* __restrict__ ranges, const int32_t* __restrict__ point_list,
     const float4* __restrict__ rec, const float* __restrict__ k, float dxy2, const float2* __restrict__ grad, int W,
@@ -571,7 +583,8 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
                 const float raw_power = -0.5f * mahal;
                 const float G = __expf(fmaxf(raw_power, -50.0f));
                 const float alpha = opac * G;
-                const float base = 0.5f * curv * mahal * ar * dxy2;
+                const float d2 = dx * dx + dy * dy;
+                const float base = ISO ? 0.5f * curv * d2 * dxy2 : 0.5f * curv * mahal * ar * dxy2;
                 const int p = yy * kTile + xx;
                 float S_alpha = 0.f, S_base = 0.f;
 #pragma unroll
@@ -588,9 +601,18 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
                     S_base = fmaf(kc[c], aph, S_base);
                 }
                 const float dpow = (raw_power >= -50.0f) ? -0.5f : 0.0f;
-                const float dmahal = S_alpha * opac * G * dpow + S_base * kb;
-                dcv = fmaf(S_base, 0.5f * mahal * ar * dxy2, dcv);
-                dar = fmaf(S_base, 0.5f * curv * mahal * dxy2, dar);
+                float dmahal;
+                if (ISO) {
+                    // the phase reaches the means directly: dbase/dmu = c dxy2 (mu - r)
+                    dmahal = S_alpha * opac * G * dpow;
+                    dcv = fmaf(S_base, 0.5f * d2 * dxy2, dcv);
+                    dmx = fmaf(S_base * curv * dxy2, dx, dmx);
+                    dmy = fmaf(S_base * curv * dxy2, dy, dmy);
+                } else {
+                    dmahal = S_alpha * opac * G * dpow + S_base * kb;
+                    dcv = fmaf(S_base, 0.5f * mahal * ar * dxy2, dcv);
+                    dar = fmaf(S_base, 0.5f * curv * mahal * dxy2, dar);
+                }
                 d00 = fmaf(dmahal, dx * dx, d00);
                 d01 = fmaf(dmahal, 2.0f * dx * dy, d01);
                 d11 = fmaf(dmahal, dy * dy, d11);
@@ -617,16 +639,26 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
 
 void launch_splat_backward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
                            const float* records, const float* k, float dxy2, const float2* grad,
-                           const SplatGrads& out, cudaStream_t stream) {
+                           const SplatGrads& out, cudaStream_t stream, bool iso) {
     const int width = rule.width, height = rule.height;
     const int gx = (width + kTile - 1) / kTile, gy = (height + kTile - 1) / kTile;
     const float4* rec = reinterpret_cast<const float4*>(records);
-    if (channels == 1)
-        splat_backward_kernel<1><<<gx * gy, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2, grad,
-                                                                      width, height, gx, out);
-    else
-        splat_backward_kernel<3><<<gx * gy, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2, grad,
-                                                                      width, height, gx, out);
+    const dim3 grid(gx * gy);
+    if (channels == 1) {
+        if (iso)
+            splat_backward_kernel<1, true><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
+                                                                             grad, width, height, gx, out);
+        else
+            splat_backward_kernel<1, false><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
+                                                                              grad, width, height, gx, out);
+    } else {
+        if (iso)
+            splat_backward_kernel<3, true><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
+                                                                             grad, width, height, gx, out);
+        else
+            splat_backward_kernel<3, false><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
+                                                                              grad, width, height, gx, out);
+    }
 }
 
 }  // namespace cvqpg
@@ -664,6 +696,7 @@ extern "C" int cvqpg_render_workspace_size(int n, int width, int height, int pai
 }
 
 extern "C" int cvqpg_render_num_lists(int cull_mode, int width, int height) {
+    cull_mode &= ~CVQPG_PHASE_ISO;
     if (cull_mode < 0 || cull_mode > 2 || width <= 0 || height <= 0) return -1;
     BinRule r = make_bin_rule(cull_mode, width, height, nullptr, nullptr);
     return bin_rule_lists(r);
@@ -677,6 +710,8 @@ extern "C" int cvqpg_render_forward_cull(const float* means_2d, const float* inv
                                          int pair_capacity, int32_t* ranges, int32_t* pair_count, void* workspace,
                                          size_t workspace_bytes, void* stream_) {
     if (channels != 1 && channels != 3) return CVQPG_ERR_CHANNELS;
+    const bool iso = (cull_mode & CVQPG_PHASE_ISO) != 0;
+    cull_mode &= ~CVQPG_PHASE_ISO;
     if (n < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || cull_mode < 0 || cull_mode > 2)
         return CVQPG_ERR_ARG;
     if (!k || !out_field || !ranges || !pair_count) return CVQPG_ERR_ARG;
@@ -695,7 +730,7 @@ extern "C" int cvqpg_render_forward_cull(const float* means_2d, const float* inv
     launch_tile_count(rule, rec, n, ws.tiles_touched, stream);
     launch_binning(rule, rec, ws, point_list, ranges, pair_count, stream);
     launch_splat_forward(channels, rule, ranges, point_list, rec, k, dxy2, reinterpret_cast<float2*>(out_field),
-                         stream);
+                         stream, iso);
     return launch_status();
 }
 
@@ -726,6 +761,8 @@ extern "C" int cvqpg_render_backward_cull(const float* grad_field, const float* 
                                           float* d_curvature, float* d_area, void* workspace,
                                           size_t workspace_bytes, void* stream_) {
     if (channels != 1 && channels != 3) return CVQPG_ERR_CHANNELS;
+    const bool iso = (cull_mode & CVQPG_PHASE_ISO) != 0;
+    cull_mode &= ~CVQPG_PHASE_ISO;
     if (n < 0 || width <= 0 || height <= 0 || cull_mode < 0 || cull_mode > 2) return CVQPG_ERR_ARG;
     if (n == 0) return CVQPG_OK;
     if (!grad_field || !means_2d || !inv_cov || !colours || !phase || !opacities || !curvature || !area || !k ||
@@ -750,7 +787,7 @@ extern "C" int cvqpg_render_backward_cull(const float* grad_field, const float* 
     BinRule rule = make_bin_rule(cull_mode, width, height, nullptr, nullptr);
     SplatGrads out{d_means, d_inv_cov, d_colours, d_phase, d_opacities, d_curvature, d_area};
     launch_splat_backward(C, rule, ranges, point_list, rec, k, dxy2, reinterpret_cast<const float2*>(grad_field),
-                          out, stream);
+                          out, stream, iso);
     return launch_status();
 }
 

@@ -67,7 +67,7 @@ void launch_binning(const BinRule& rule, const float* records, const BinWorkspac
                     int32_t* ranges, int32_t* pair_count, cudaStream_t stream);
 
 void launch_splat_forward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
-                          const float* records, const float* k, float dxy2, float2* out, cudaStream_t stream);
+                          const float* records, const float* k, float dxy2, float2* out, cudaStream_t stream, bool iso = false);
 
 // Gradient outputs in the reference SoA layout; they are accumulated with
 // atomics and must be zeroed beforehand.
@@ -83,7 +83,7 @@ struct SplatGrads {
 
 void launch_splat_backward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
                            const float* records, const float* k, float dxy2, const float2* grad,
-                           const SplatGrads& out, cudaStream_t stream);
+                           const SplatGrads& out, cudaStream_t stream, bool iso = false);
 
 // Tile rectangle of a Gaussian, written with the exact float operation order
 // of the reference getRect (cuda/forward.cu:8-13) so that the per-tile lists

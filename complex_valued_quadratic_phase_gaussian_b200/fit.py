@@ -71,6 +71,7 @@ class FitConfig:
     split_ratio: float = 1.0
     seed: int = 0
     cull: int = CULL_CUDA16_5SIGMA
+    phase_iso: bool = False                  # isotropic quadratic phase (--phase_iso, model_2d_gaussian_rgb.py:356-359)
     pair_capacity: Optional[int] = None
     inject_noise: bool = True
     history_len: int = 4096
@@ -182,7 +183,7 @@ class Fitter:
         p.pad_height, p.pad_width = int(pad[0]), int(pad[1])
         p.num_gaussians = N
         p.pair_capacity = int(cfg.pair_capacity if cfg.pair_capacity else max(1 << 16, 24 * N))
-        p.cull_mode = int(cfg.cull)
+        p.cull_mode = int(cfg.cull) | (0x100 if cfg.phase_iso else 0)  # CVQPG_PHASE_ISO
         flat = cfg.primitive == "flat"
         p.curv_mode = 0 if flat else CURV_MODES[cfg.curv_mode]
         p.curv_trainable = 0 if flat else 1

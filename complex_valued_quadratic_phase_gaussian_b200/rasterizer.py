@@ -22,6 +22,7 @@ from . import _lib
 CULL_CUDA16_5SIGMA = 0
 CULL_TORCH64_3SIGMA = 1
 CULL_NONE = 2
+PHASE_ISO = 0x100  # OR-ed into the cull mode: isotropic quadratic phase (reference --phase_iso)
 
 _capacity_hint = {}
 
@@ -43,8 +44,11 @@ def _check_channels(c):
 
 
 def render_forward(means_2d, inv_cov, colours, phase, opacities, curvature, area, k, dxy2, width, height,
-                   cull=CULL_CUDA16_5SIGMA, radii=None, radius3=None):
+                   cull=CULL_CUDA16_5SIGMA, radii=None, radius3=None, phase_iso=False):
     """Run binning + splat. Returns (field complex64 [C,H,W], point_list, ranges).
+
+    phase_iso: isotropic quadratic phase 0.5 c |r - mu|^2 dxy2 (the torch renderer's
+    --phase_iso) instead of the Mahalanobis form 0.5 c m area dxy2.
 
     ``point_list`` holds exactly the produced pairs (the reference's
     ``total_pairs``; a single zero when there are none, cuda/raster.cu:72-75).
@@ -77,7 +81,8 @@ def render_forward(means_2d, inv_cov, colours, phase, opacities, curvature, area
             point_list = torch.empty(max(cap, 1), dtype=torch.int32, device=dev)
             _lib.check(lib.cvqpg_render_forward_cull(
                 _lib.ptr(means_2d), _lib.ptr(inv_cov), _lib.ptr(colours), _lib.ptr(phase), _lib.ptr(opacities),
-                _lib.ptr(curvature), _lib.ptr(area), int(cull), _lib.ptr(radii), _lib.ptr(radius3),
+                _lib.ptr(curvature), _lib.ptr(area), int(cull) | (PHASE_ISO if phase_iso else 0), _lib.ptr(radii),
+                _lib.ptr(radius3),
                 _lib.ptr(k), float(dxy2), n, int(width), int(height), c, _lib.ptr(torch.view_as_real(out)),
                 _lib.ptr(point_list), cap, _lib.ptr(ranges), _lib.ptr(pair_count), _lib.ptr(ws), ws.numel(),
                 _lib.stream_of(dev)), "qpf_render_forward")
@@ -94,7 +99,7 @@ def render_forward(means_2d, inv_cov, colours, phase, opacities, curvature, area
 
 
 def render_backward(grad_field, means_2d, inv_cov, colours, phase, opacities, curvature, area, k, point_list,
-                    ranges, dxy2, width, height, cull=CULL_CUDA16_5SIGMA):
+                    ranges, dxy2, width, height, cull=CULL_CUDA16_5SIGMA, phase_iso=False):
     """Adjoint of render_forward; returns the 7 input gradients."""
     n = means_2d.size(0)
     c = colours.size(1) if colours.dim() == 2 else 1
@@ -115,7 +120,8 @@ def render_backward(grad_field, means_2d, inv_cov, colours, phase, opacities, cu
         ws = _lib.workspace(_lib.size_query(lib.cvqpg_render_backward_workspace_size, n), dev)
         _lib.check(lib.cvqpg_render_backward_cull(
             _lib.ptr(torch.view_as_real(g)), _lib.ptr(means_2d), _lib.ptr(inv_cov), _lib.ptr(colours),
-            _lib.ptr(phase), _lib.ptr(opacities), _lib.ptr(curvature), _lib.ptr(area), _lib.ptr(k), int(cull),
+            _lib.ptr(phase), _lib.ptr(opacities), _lib.ptr(curvature), _lib.ptr(area), _lib.ptr(k),
+            int(cull) | (PHASE_ISO if phase_iso else 0),
             _lib.ptr(point_list), _lib.ptr(ranges), float(dxy2), n, int(width), int(height), c,
             _lib.ptr(d_means), _lib.ptr(d_inv), _lib.ptr(d_col), _lib.ptr(d_ph), _lib.ptr(d_op), _lib.ptr(d_cv),
             _lib.ptr(d_ar), _lib.ptr(ws), ws.numel(), _lib.stream_of(dev)), "qpf_render_backward")
@@ -182,24 +188,24 @@ class QPFRenderCull(Function):
 
     @staticmethod
     def forward(ctx, means_2d, inv_cov, colours, phase, opacities, curvature, area, k, dxy2, width, height, cull,
-                radii, radius3):
+                radii, radius3, phase_iso=False):
         args = [t.contiguous() for t in (means_2d, inv_cov, colours, phase, opacities, curvature, area)]
         kk = k.contiguous()
         out, point_list, ranges = render_forward(
             *args, kk, dxy2, width, height, cull,
             radii=None if radii is None else radii.contiguous().int(),
-            radius3=None if radius3 is None else radius3.detach().contiguous().float())
+            radius3=None if radius3 is None else radius3.detach().contiguous().float(), phase_iso=phase_iso)
         ctx.save_for_backward(*args, kk, point_list, ranges)
-        ctx.cfg = (float(dxy2), int(width), int(height), int(cull))
+        ctx.cfg = (float(dxy2), int(width), int(height), int(cull), bool(phase_iso))
         return out
 
     @staticmethod
     def backward(ctx, grad_out):
         (means, inv_cov, colours, phase, opac, curv, area, k, point_list, ranges) = ctx.saved_tensors
-        dxy2, w, h, cull = ctx.cfg
+        dxy2, w, h, cull, iso = ctx.cfg
         d = render_backward(grad_out, means, inv_cov, colours, phase, opac, curv, area, k, point_list, ranges,
-                            dxy2, w, h, cull)
-        return (d[0], d[1], d[2], d[3], d[4], d[5], d[6]) + (None,) * 7
+                            dxy2, w, h, cull, phase_iso=iso)
+        return (d[0], d[1], d[2], d[3], d[4], d[5], d[6]) + (None,) * 8
 
 
 def qpf_render(means_2d, inv_cov, colours, phase, opacities, curvature, area, radii, k, dxy2, width, height):
@@ -214,7 +220,8 @@ def qpf_render(means_2d, inv_cov, colours, phase, opacities, curvature, area, ra
 
 
 def qpf_render_cull(means_2d, inv_cov, colours, phase, opacities, curvature, area, k, dxy2, width, height,
-                    cull=CULL_CUDA16_5SIGMA, radii=None, radius3=None):
-    """qpf_render with an explicit culling rule (for like-with-like parity checks)."""
+                    cull=CULL_CUDA16_5SIGMA, radii=None, radius3=None, phase_iso=False):
+    """qpf_render with an explicit culling rule (for like-with-like parity checks) and optionally the
+    isotropic quadratic phase of the torch renderer's --phase_iso (model_2d_gaussian_rgb.py:356-359)."""
     return QPFRenderCull.apply(means_2d, inv_cov, colours, phase, opacities, curvature, area, k, dxy2, width,
-                               height, cull, radii, radius3)
+                               height, cull, radii, radius3, phase_iso)

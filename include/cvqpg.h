@@ -46,6 +46,11 @@ extern "C" {
 #define CVQPG_CULL_CUDA16_5SIGMA 0  /* reference CUDA renderer: 16-px tiles, int radius rect */
 #define CVQPG_CULL_TORCH64_3SIGMA 1 /* reference torch renderer: 64-px tiles, 3-sigma circle */
 #define CVQPG_CULL_NONE 2           /* every Gaussian at every pixel                          */
+/* OR-ed into a cull mode: the isotropic quadratic phase 0.5*c*|r-mu|^2*dxy2 of the
+ * torch renderer's --phase_iso (model_2d_gaussian_rgb.py:356-359) instead of the
+ * Mahalanobis form 0.5*c*m*area*dxy2 (:360-363); the reference CUDA renderer
+ * rejects --phase_iso (model_2d_gaussian_rgb.py:263-265), this one supports it. */
+#define CVQPG_PHASE_ISO 0x100
 
 /* Human-readable text of a status code. */
 CVQPG_API const char* cvqpg_status_string(int status);

@@ -124,8 +124,12 @@ def _as64(*arrs):
 
 
 def splat_forward(means, inv_cov, colours, phase, opac, curv, area, k, dxy2, W, H, cull=CULL_NONE,
-                  point_list=None, ranges=None, chunk=512):
-    """Complex field [C,H,W] (complex128). With cull=CULL_NONE every Gaussian hits every pixel."""
+                  point_list=None, ranges=None, chunk=512, phase_iso=False):
+    """Complex field [C,H,W] (complex128). With cull=CULL_NONE every Gaussian hits every pixel.
+
+    phase_iso: the isotropic quadratic phase 0.5 c |r - mu|^2 dxy2 of the torch
+    renderer's --phase_iso (model_2d_gaussian_rgb.py:356-359) instead of the
+    Mahalanobis form 0.5 c m area dxy2 (model_2d_gaussian_rgb.py:360-363)."""
     means, inv_cov, colours, phase, opac, curv, area, k = _as64(means, inv_cov, colours, phase, opac, curv, area, k)
     C = colours.shape[1]
     n = means.shape[0]
@@ -150,7 +154,10 @@ def splat_forward(means, inv_cov, colours, phase, opac, curv, area, k, dxy2, W, 
                 mahal = dx * (i00 * dx + i01 * dy) + dy * (i01 * dx + i11 * dy)
                 G = np.exp(np.maximum(-0.5 * mahal, -50.0))
                 alpha = opac[g, None] * G
-                base = 0.5 * curv[g, None] * mahal * area[g, None] * dxy2
+                if phase_iso:
+                    base = 0.5 * curv[g, None] * (dx * dx + dy * dy) * dxy2
+                else:
+                    base = 0.5 * curv[g, None] * mahal * area[g, None] * dxy2
                 for c in range(C):
                     ph = phase[g, c:c + 1] + k[c] * base
                     acc[c] += np.sum(colours[g, c:c + 1] * alpha * np.exp(1j * ph), axis=0)
@@ -161,7 +168,7 @@ def splat_forward(means, inv_cov, colours, phase, opac, curv, area, k, dxy2, W, 
 
 
 def splat_backward(grad, means, inv_cov, colours, phase, opac, curv, area, k, dxy2, W, H, cull=CULL_NONE,
-                   point_list=None, ranges=None, chunk=512):
+                   point_list=None, ranges=None, chunk=512, phase_iso=False):
     """Gradients (d_means, d_inv, d_col, d_ph, d_op, d_cv, d_ar) in float64.
 
     grad is dL/dU as complex (real part dL/dRe, imaginary part dL/dIm).
@@ -203,7 +210,8 @@ def splat_backward(grad, means, inv_cov, colours, phase, opac, curv, area, k, dx
                 alpha = o * G
                 cv = curv[g, None]
                 ar = area[g, None]
-                base = 0.5 * cv * mahal * ar * dxy2
+                d2 = dx * dx + dy * dy
+                base = 0.5 * cv * d2 * dxy2 if phase_iso else 0.5 * cv * mahal * ar * dxy2
                 S_alpha = np.zeros_like(mahal)
                 S_base = np.zeros_like(mahal)
                 for c in range(C):
@@ -219,9 +227,16 @@ def splat_backward(grad, means, inv_cov, colours, phase, opac, curv, area, k, dx
                     S_alpha += A * proj_c
                     S_base += k[c] * dph
                 dpow = np.where(raw_power >= -50.0, -0.5, 0.0)
-                dmahal = S_alpha * o * G * dpow + S_base * 0.5 * cv * ar * dxy2
-                d_cv[g] += np.sum(S_base * 0.5 * mahal * ar * dxy2, axis=1)
-                d_ar[g] += np.sum(S_base * 0.5 * cv * mahal * dxy2, axis=1)
+                if phase_iso:
+                    dmahal = S_alpha * o * G * dpow
+                    d_cv[g] += np.sum(S_base * 0.5 * d2 * dxy2, axis=1)
+                    # the phase depends on the means directly: dbase/dmu = c dxy2 (mu - r)
+                    d_means[g, 0] += np.sum(S_base * cv * dxy2 * dx, axis=1)
+                    d_means[g, 1] += np.sum(S_base * cv * dxy2 * dy, axis=1)
+                else:
+                    dmahal = S_alpha * o * G * dpow + S_base * 0.5 * cv * ar * dxy2
+                    d_cv[g] += np.sum(S_base * 0.5 * mahal * ar * dxy2, axis=1)
+                    d_ar[g] += np.sum(S_base * 0.5 * cv * mahal * dxy2, axis=1)
                 d_inv[g, 0] += np.sum(dmahal * dx * dx, axis=1)
                 d_inv[g, 1] += np.sum(dmahal * 2.0 * dx * dy, axis=1)
                 d_inv[g, 2] += np.sum(dmahal * dy * dy, axis=1)

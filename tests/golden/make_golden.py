@@ -120,10 +120,10 @@ def golden_splat(C, name, seed, n=200, W=50, H=40):
                         **p, **grads)
 
 
-def _args_prop(C, pad_size, renderer="torch"):
+def _args_prop(C, pad_size, renderer="torch", phase_iso=False):
     wl = WAVELENGTHS if C == 3 else WAVELENGTHS[:1]
     return Namespace(wavelengths=list(wl), pixel_pitch=PITCH, pad_size=list(pad_size), tile_size=64, gauss_batch=1024,
-                     phase_iso=False, grad_ckpt=False, renderer=renderer, curv_nyquist=0.9)
+                     phase_iso=phase_iso, grad_ckpt=False, renderer=renderer, curv_nyquist=0.9)
 
 
 def raw_params(rng, n, W, H, C, curv_scale=1.0):
@@ -191,13 +191,15 @@ def golden_preprocess(C, name, seed, n=300, W=96, H=80):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), W=W, H=H, C=C, **raw, **out)
 
 
-def golden_torch_renderer(C, name, seed, n=400, W=160, H=112, pad=(176, 224)):
-    """The reference torch tile renderer (3-sigma 64-px culling) + soft_window_pad, with gradients."""
+def golden_torch_renderer(C, name, seed, n=400, W=160, H=112, pad=(176, 224), phase_iso=False):
+    """The reference torch tile renderer (3-sigma 64-px culling) + soft_window_pad, with gradients.
+
+    phase_iso=True renders the isotropic quadratic phase of --phase_iso."""
     model = load_by_path(f"ref_model_{C}", ref("model_2d_gaussian_rgb.py" if C == 3 else
                                               "model_2d_gaussian_grayscale.py"))
     rng = np.random.default_rng(seed)
     raw = raw_params(rng, n, W, H, C, curv_scale=2.0)
-    ap = _args_prop(C, pad)
+    ap = _args_prop(C, pad, phase_iso=phase_iso)
     g = _make_gaussians(model, raw, W, H, C, ap, "scale_aware")
     with torch.no_grad():
         scales, rotation, phase, opac, means, curv = g.apply_activations()
@@ -373,6 +375,7 @@ GOLDENS = {
     "preprocess_gray": lambda: golden_preprocess(1, "preprocess_gray", 22),
     "torch_renderer_rgb": lambda: golden_torch_renderer(3, "torch_renderer_rgb", 31),
     "torch_renderer_gray": lambda: golden_torch_renderer(1, "torch_renderer_gray", 32),
+    "torch_renderer_iso_rgb": lambda: golden_torch_renderer(3, "torch_renderer_iso_rgb", 33, phase_iso=True),
     # 2pH = 176 = 16*11, 2pW = 208 = 16*13, 3 planes, aperture wide open (train default 10*max(img))
     "propagate_rgb": lambda: golden_propagate(3, "propagate_rgb", 41, 40, 56, 88, 104, 3, 1e-3, 1e-3, 560),
     # 2pH = 2pW = 120 = 8*3*5: band limit active (z = 5 cm) and a small Fourier aperture

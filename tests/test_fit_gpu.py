@@ -127,3 +127,18 @@ def test_pair_capacity_overflow_is_reported():
     f.step()
     torch.cuda.synchronize()
     assert f.overflowed()
+
+
+def test_isotropic_phase_fit_reduces_loss():
+    """The fused iteration with --phase_iso (torch-renderer cull rule, isotropic QPF) trains."""
+    from complex_valued_quadratic_phase_gaussian_b200 import learned as L
+    from complex_valued_quadratic_phase_gaussian_b200.fit import CULL_TORCH64_3SIGMA, Fitter, synthetic_init
+    H, W = 64, 96
+    img, depth, targets, q = L.make_scene(H, W, 3)
+    cfg = L.scene_config(H, W, 60, seed=3, cull=CULL_TORCH64_3SIGMA, phase_iso=True, autotune=False)
+    f = Fitter(cfg, targets, q, init=synthetic_init(cfg, 3))
+    l0 = f.evaluate()["loss"]
+    f.run(60)
+    ev = f.evaluate()
+    assert np.isfinite(ev["loss"]) and ev["loss"] < 0.7 * l0
+    assert not f.overflowed()

@@ -104,3 +104,39 @@ def test_oracle_preprocess_matches_reference(golden, name, mode):
             assert np.linalg.norm(grads[key]) == 0, key
             continue
         assert rel_l2(grads[key], ref) < 2e-5, key
+
+
+def test_oracle_isotropic_phase_matches_reference_torch_renderer(golden):
+    """--phase_iso: field of the reference torch renderer (isotropic QPF) within 2e-6 (float32 vs float64)."""
+    g = golden("torch_renderer_iso_rgb")
+    W, H = int(g["W"]), int(g["H"])
+    pl, ranges = osp.bin_lists(g["act_means"], W, H, osp.CULL_TORCH64_3SIGMA, radius3=g["act_radius3"])
+    out = osp.splat_forward(g["act_means"], g["act_inv_cov"], g["colours"], g["act_phase"], g["act_opac"],
+                            g["act_curv"], g["act_area"], g["act_k"], float(g["act_dxy2"]), W, H,
+                            cull=osp.CULL_TORCH64_3SIGMA, point_list=pl, ranges=ranges, phase_iso=True)
+    assert rel_l2(out, g["field"]) < 2e-6
+
+
+def test_oracle_isotropic_adjoint_matches_finite_differences():
+    rng = np.random.default_rng(8)
+    n, W, H, C = 6, 20, 18, 3
+    means = np.stack([rng.uniform(4, W - 4, n), rng.uniform(4, H - 4, n)], 1)
+    inv = np.stack([rng.uniform(0.1, 0.3, n), rng.uniform(-0.05, 0.05, n), rng.uniform(0.1, 0.3, n)], 1)
+    col, ph = rng.uniform(0, 1, (n, C)), rng.uniform(0, 6, (n, C))
+    op, cv, ar = rng.uniform(0.3, 0.9, n), rng.normal(0, 3e4, n), rng.uniform(2, 6, n)
+    k = 2 * np.pi / np.array([639e-9, 515e-9, 473e-9])
+    dxy2 = 3.74e-6 ** 2
+    G = rng.normal(size=(C, H, W)) + 1j * rng.normal(size=(C, H, W))
+    args = [means, inv, col, ph, op, cv, ar]
+    loss = lambda a: float(np.sum((osp.splat_forward(*a, k, dxy2, W, H, phase_iso=True) * np.conj(G)).real))
+    grads = osp.splat_backward(G, *args, k, dxy2, W, H, phase_iso=True)
+    for ai, (arr, gr) in enumerate(zip(args, grads)):
+        for idx in [(0,) * arr.ndim, tuple(d - 1 for d in arr.shape)]:
+            h = 1e-6 * max(1.0, abs(arr[idx]))
+            ap = [a.copy() for a in args]
+            am = [a.copy() for a in args]
+            ap[ai][idx] += h
+            am[ai][idx] -= h
+            fd = (loss(ap) - loss(am)) / (2 * h)
+            assert abs(gr[idx] - fd) <= 1e-5 * max(1.0, abs(fd)), (ai, idx, gr[idx], fd)
+    assert np.all(grads[6] == 0)  # the area does not enter the isotropic phase

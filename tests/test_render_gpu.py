@@ -153,3 +153,34 @@ def test_reference_error_behaviour():
     with pytest.raises(RuntimeError, match="num_channels entries"):
         pkg.ext().qpf_render_forward(t(n, 2), t(n, 3), t(n, 1), t(n, 1), t(n), t(n), t(n), radii, t(3), 1.0, 8, 8,
                                      1)
+
+
+def test_isotropic_phase_vs_reference_torch_renderer(golden):
+    """--phase_iso (the reference supports it only in its torch renderer): field within 1e-4 of that
+    renderer, within 1e-5 of the float64 oracle; adjoint within 1e-4 of the oracle, no area gradient."""
+    from complex_valued_quadratic_phase_gaussian_b200 import rasterizer as R
+    g = golden("torch_renderer_iso_rgb")
+    W, H = int(g["W"]), int(g["H"])
+    names = ("act_means", "act_inv_cov", "colours", "act_phase", "act_opac", "act_curv", "act_area")
+    ins = [torch.from_numpy(np.ascontiguousarray(g[k], dtype=np.float32)).cuda().requires_grad_(True) for k in names]
+    k = torch.from_numpy(g["act_k"]).cuda()
+    r3 = torch.from_numpy(g["act_radius3"]).cuda()
+    out = R.qpf_render_cull(*ins, k, float(g["act_dxy2"]), W, H, cull=R.CULL_TORCH64_3SIGMA, radius3=r3,
+                            phase_iso=True)
+    got = out.detach().cpu().numpy()
+    assert rel_l2(got, g["field"]) < 1e-4
+    args = [g[k_] for k_ in names]
+    pl, ranges = osp.bin_lists(g["act_means"], W, H, osp.CULL_TORCH64_3SIGMA, radius3=g["act_radius3"])
+    ref = osp.splat_forward(*args, g["act_k"], float(g["act_dxy2"]), W, H, cull=osp.CULL_TORCH64_3SIGMA,
+                            point_list=pl, ranges=ranges, phase_iso=True)
+    assert rel_l2(got, ref) < 1e-5
+    gw = g["grad_field"]  # any fixed field-shaped weight
+    gt = torch.from_numpy(gw.astype(np.complex64)).cuda()
+    ((out.real * gt.real).sum() + (out.imag * gt.imag).sum()).backward()
+    dref = osp.splat_backward(gw, *args, g["act_k"], float(g["act_dxy2"]), W, H, cull=osp.CULL_TORCH64_3SIGMA,
+                              point_list=pl, ranges=ranges, phase_iso=True)
+    for name, t, b in zip(names, ins, dref):
+        if name == "act_area":
+            assert torch.count_nonzero(t.grad).item() == 0
+            continue
+        assert rel_l2(t.grad.cpu().numpy(), b) < 1e-4, name
