@@ -206,7 +206,7 @@ def build_scene(wl, seed, device):
         img, depth = scenes.rgb_blobs(wl["H"], wl["W"], seed=seed)
     else:
         img, depth = scenes.grayscale_blobs(wl["H"], wl["W"], seed=seed)
-    targets, q = scenes.multiplane_targets(img, depth, wl["P"], device=device)
+    targets, q = scenes.multiplane_targets_device(img, depth, wl["P"], device=device)
     return img, depth, targets, q
 
 

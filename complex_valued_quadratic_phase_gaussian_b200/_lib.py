@@ -45,6 +45,9 @@ _SIGNATURES = {
     "cvqpg_loss_workspace_size": [_p, _psz],
     "cvqpg_loss_target_range": [_p, _i, _i, _i, _i, _p, _p, _sz, _p],
     "cvqpg_loss_forward_backward": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
+    "cvqpg_targets_workspace_size": [_i, _i, _i, _i, _psz],
+    "cvqpg_targets_synthesize": [_p, _p, _i, _i, _i, _i, _i, _f, _f, _p, _p, _p, _sz, _p],
+    "cvqpg_poh_encode": [_p, _p, _sz, _p, _p, _p, _p],
     "cvqpg_gemm_bf16_tn": [_p, _i, _p, _i, _i, _i, _i, _p, _i, _p, _p],
     "cvqpg_mlp_weights_size": [_p, _psz],
     "cvqpg_mlp_workspace_size": [_p, _psz],

@@ -29,7 +29,7 @@ import torch
 from .batch import BatchedFitter, FitJob
 from .fit import FitConfig, Fitter, synthetic_init
 from .mlp import TileMLP
-from .scenes import multiplane_targets, rgb_crop_like_1080p
+from .scenes import multiplane_targets_device, rgb_crop_like_1080p
 
 TILE = 16
 SLOTS = 12
@@ -140,7 +140,7 @@ def scene_config(H, W, iters, seed=0, **kw):
 
 def make_scene(H, W, seed, device="cuda"):
     img, depth = rgb_crop_like_1080p(H, W, seed=seed)
-    targets, q = multiplane_targets(img, depth, 3, device=device)
+    targets, q = multiplane_targets_device(img, depth, 3, device=device)
     return img, depth, targets, q
 
 

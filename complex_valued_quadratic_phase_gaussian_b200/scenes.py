@@ -21,6 +21,8 @@ import numpy as np
 import torch
 import torch.nn.functional as F
 
+from . import _lib
+
 
 def _fbm(rng, H, W, beta=1.0):
     """1/f^beta noise field in [0, 1] (spectral synthesis, seeded)."""
@@ -127,3 +129,20 @@ def multiplane_targets(image, depth, num_planes, blur_size=20, blur_ratio=8, spl
                     acc = acc + blurred[key] * masks[j]
             targets[i, ch] = acc
     return targets.contiguous(), q.to(torch.uint8).contiguous()
+
+
+def multiplane_targets_device(image, depth, num_planes, blur_size=20, blur_ratio=8, split_ratio=1.0, device="cuda"):
+    """Per-plane defocus targets [P,C,H,W] and plane index [H,W] with the library's kernels
+    (cvqpg_targets_synthesize): the same arithmetic as ``multiplane_targets``, on the GPU."""
+    dev = torch.device(device)
+    img = torch.as_tensor(image, dtype=torch.float32).to(dev).contiguous()
+    C, H, W = img.shape
+    d = torch.as_tensor(depth, dtype=torch.float32).to(dev).reshape(H, W).contiguous()
+    targets = torch.empty((num_planes, C, H, W), dtype=torch.float32, device=dev)
+    q = torch.empty((H, W), dtype=torch.uint8, device=dev)
+    lib = _lib.lib()
+    ws = _lib.workspace(_lib.size_query(lib.cvqpg_targets_workspace_size, C, H, W, int(num_planes)), dev)
+    _lib.check(lib.cvqpg_targets_synthesize(_lib.ptr(img), _lib.ptr(d), C, H, W, int(num_planes), int(blur_size),
+                                            float(blur_ratio), float(split_ratio), _lib.ptr(targets), _lib.ptr(q),
+                                            _lib.ptr(ws), ws.numel(), _lib.stream_of(dev)), "cvqpg_targets_synthesize")
+    return targets, q

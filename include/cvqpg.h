@@ -423,6 +423,31 @@ CVQPG_API int cvqpg_mlp_train_step(const cvqpg_mlp_params* prm, float* weights, 
                                    const float* X, const float* T, const float* out_weight, float* loss,
                                    void* workspace, size_t workspace_bytes, int* status, void* stream);
 
+/* ---- multi-plane defocus targets (once per scene) --------------------------
+ *
+ * Replaces set_targets + add_defocus_blur (utils/propagator.py:361-415) with
+ * the factory settings of utils/data_utils.py:66-82 (blur_size 20, blur_ratio 8):
+ * plane_index = round(depth^r * (P-1)) (r = split_ratio when P == 2, else 1),
+ * targets[i][c] = sum_j [sum(image_c * M_j) > 0] * (K_{int(|i-j| blur_ratio)} * image_c) * M_j,
+ * M_j = [plane_index == j], K_s the normalised (blur_size+1)^2 Gaussian (an
+ * impulse for s = 0), zero-padded 'same'. image [C,H,W], depth [H,W] in [0,1],
+ * targets [P,C,H,W], plane_index [H,W]; planes <= 8. */
+CVQPG_API int cvqpg_targets_workspace_size(int channels, int height, int width, int planes, size_t* bytes);
+CVQPG_API int cvqpg_targets_synthesize(const float* image, const float* depth, int channels, int height, int width,
+                                       int planes, int blur_size, float blur_ratio, float split_ratio,
+                                       float* targets, uint8_t* plane_index, void* workspace,
+                                       size_t workspace_bytes, void* stream);
+
+/* ---- phase-only hologram export (export_poh.py:110-119, 175-194) -----------
+ *
+ * From the splat field [C,H,W] (prm->input_mode 0, tables of cvqpg_blasm_setup):
+ * soft window pad + amplitude clamp -> DPAC (phase -/+ arccos(amplitude) on a
+ * checkerboard, minus where y + x is even) -> 8-bit levels [C,pH,pW]
+ * (round(poh / 2pi * 256) mod 256). phase_field (nullable, complex [C,pH,pW]):
+ * exp(i 2 pi level / 256), ready for cvqpg_blasm_forward with input_mode 1. */
+CVQPG_API int cvqpg_poh_encode(const cvqpg_blasm_params* prm, const void* tables, size_t table_bytes,
+                               const float* field, uint8_t* levels, float* phase_field, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

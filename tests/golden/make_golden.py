@@ -282,6 +282,25 @@ class _MeansCosine:
             self.optimizer.param_groups[gi]["lr"] = self.sch.get_last_lr()[i]
 
 
+def golden_targets(C, name, seed, H=72, W=104, P=4):
+    """Multi-plane defocus targets of the reference loss (utils/propagator.py:361-415) via get_targets()."""
+    from complex_valued_quadratic_phase_gaussian_b200 import scenes as sc
+    prop_mod = load_by_path("ref_propagator", ref("utils/propagator.py"))
+    img, depth = sc.rgb_blobs(H, W, seed=seed, num_blobs=60) if C == 3 else sc.grayscale_blobs(H, W, seed=seed)
+    img = img.copy()
+    img[:, :, :6] = 0.0   # a zero column band: exercises planes whose masked image sums to zero
+    depth = 0.8 * depth  # planes 0..2 over the scene
+    depth[:, :6] = 0.99   # ... and plane 3 only on the zero band, so its masked image sums to zero
+    loss_fn = prop_mod.multiplane_loss_odak(target_image=torch.from_numpy(img),
+                                            target_depth=torch.from_numpy(depth)[None], target_blur_size=20,
+                                            number_of_planes=P, blur_ratio=8, weights=[1.0, 1.0, 1.0, 0.0],
+                                            scheme="defocus", reduction="mean", split_ratio=1.0, device="cpu")
+    targets, masks, qdepth = loss_fn.get_targets()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), image=img, depth=depth, P=P,
+                        targets=targets.numpy().astype(np.float32),
+                        plane=np.rint(qdepth.numpy().reshape(H, W) * (P - 1)).astype(np.uint8))
+
+
 def golden_fit(C, name, seed, W=96, H=64, N=200, P=2, pad=(96, 128), iters=3, warmup=1, num_itrs=10,
                d_val=1e-3, vd=1e-3):
     """Iterations of the reference fit loop body (train_2d_gaussian_rgb.py:179-211) on the torch renderer."""
@@ -381,6 +400,7 @@ GOLDENS = {
     # 2pH = 2pW = 120 = 8*3*5: band limit active (z = 5 cm) and a small Fourier aperture
     "propagate_gray_bandlimit": lambda: golden_propagate(1, "propagate_gray_bandlimit", 42, 32, 32, 60, 60, 2,
                                                          5e-2, 2e-2, 40),
+    "targets_rgb": lambda: golden_targets(3, "targets_rgb", 61),
     "fit_rgb": lambda: golden_fit(3, "fit_rgb", 51),
     "fit_gray": lambda: golden_fit(1, "fit_gray", 52, P=3),
 }
