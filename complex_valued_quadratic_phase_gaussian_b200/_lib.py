@@ -54,6 +54,7 @@ _SIGNATURES = {
     "cvqpg_mlp_sync_weights": [_p, _p, _p, _sz, _p],
     "cvqpg_mlp_forward": [_p, _p, _p, _p, _p, _sz, _p, _p],
     "cvqpg_mlp_gradients": [_p, _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p],
+    "cvqpg_mlp_adam_step": [_p, _p, _p, _p, _p, _p, _sz, _p],
     "cvqpg_mlp_train_step": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p],
     "cvqpg_fit_workspace_size": [_p, _psz],
     "cvqpg_fit_setup": [_p, _p, _p, _sz],

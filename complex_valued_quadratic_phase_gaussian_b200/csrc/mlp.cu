@@ -417,6 +417,19 @@ extern "C" int cvqpg_mlp_gradients(const cvqpg_mlp_params* p, const float* weigh
     return mlp_backward_impl(d, w, T, out_weight, grads, loss, status, s);
 }
 
+extern "C" int cvqpg_mlp_adam_step(const cvqpg_mlp_params* p, float* weights, float* adam_state, int* step,
+                                   const float* grads, void* ws, size_t bytes, void* stream) {
+    MlpDims d;
+    MlpWs w;
+    int st = mlp_prepare(p, ws, bytes, &d, &w);
+    if (st) return st;
+    if (!weights || !adam_state || !step || !grads) return CVQPG_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    adam_or_sync(d, w, weights, adam_state, grads, step, p, 1, s);
+    mlp_step_kernel<<<1, 32, 0, s>>>(step);
+    return launch_status();
+}
+
 extern "C" int cvqpg_mlp_train_step(const cvqpg_mlp_params* p, float* weights, float* adam_state, int* step,
                                     const float* X, const float* T, const float* out_weight, float* loss, void* ws,
                                     size_t bytes, int* status, void* stream) {

@@ -125,6 +125,20 @@ class TileMLP:
                                            _lib.ptr(self.status), _lib.stream_of(self.device)), "cvqpg_mlp_gradients")
         return self.loss, grads
 
+    def adam_step(self, grads):
+        """One Adam step from given gradients (e.g. after a data-parallel all-reduce)."""
+        lib = _lib.lib()
+        _lib.check(lib.cvqpg_mlp_adam_step(ctypes.byref(self.prm), _lib.ptr(self.weights), _lib.ptr(self.adam),
+                                           _lib.ptr(self.step_count), _lib.ptr(grads.contiguous()), _lib.ptr(self.ws),
+                                           self.ws.numel(), _lib.stream_of(self.device)), "cvqpg_mlp_adam_step")
+
+    def data_parallel_step(self, X, T, out_weight, group=None):
+        """One data-parallel step: this rank's shard (X, T) -> gradients on the tensor cores ->
+        all-reduce weighted by rows -> the same Adam step on every rank. Returns the global loss."""
+        loss, grads = data_parallel_gradients(lambda: self.gradients(X, T, out_weight), X.shape[0], group)
+        self.adam_step(grads)
+        return loss
+
     def train_step(self, X, T, out_weight):
         """One Adam step on (X, T); returns the device loss tensor (no host sync)."""
         lib = _lib.lib()
@@ -134,6 +148,22 @@ class TileMLP:
                                             _lib.ptr(self.status), _lib.stream_of(self.device)),
                    "cvqpg_mlp_train_step")
         return self.loss
+
+
+def data_parallel_gradients(grad_fn, rows, group=None):
+    """Average per-rank gradients into the full-batch gradient of the mean loss.
+
+    grad_fn() returns (loss, grads) of this rank's shard of `rows` rows (mean over its rows).
+    The shards may differ in size: each rank's gradient and loss are weighted by its row
+    count in one all-reduce of [grads | loss | rows] (NCCL on GPUs, gloo on CPUs)."""
+    import torch.distributed as dist
+    loss, grads = grad_fn()
+    buf = torch.cat([grads.reshape(-1) * rows, torch.as_tensor(loss, dtype=grads.dtype, device=grads.device)
+                     .reshape(1) * rows, torch.tensor([float(rows)], dtype=grads.dtype, device=grads.device)])
+    if dist.is_available() and dist.is_initialized():
+        dist.all_reduce(buf, group=group)
+    total = buf[-1]
+    return buf[-2] / total, (buf[:-2] / total).reshape(grads.shape)
 
 
 def _default_init(in_dim, hidden, out_dim, seed=0):

@@ -417,6 +417,9 @@ CVQPG_API int cvqpg_mlp_forward(const cvqpg_mlp_params* prm, const float* weight
 CVQPG_API int cvqpg_mlp_gradients(const cvqpg_mlp_params* prm, const float* weights, const float* X, const float* T,
                                   const float* out_weight, float* grads, float* loss, void* workspace,
                                   size_t workspace_bytes, int* status, void* stream);
+/* Adam step from given gradients (e.g. after an all-reduce across data-parallel ranks). */
+CVQPG_API int cvqpg_mlp_adam_step(const cvqpg_mlp_params* prm, float* weights, float* adam_state, int* step,
+                                  const float* grads, void* workspace, size_t workspace_bytes, void* stream);
 /* One Adam step (state = 2 x weights: first and second moments; step = device int,
  * incremented; bias correction uses step + 1). Graph-capturable. */
 CVQPG_API int cvqpg_mlp_train_step(const cvqpg_mlp_params* prm, float* weights, float* adam_state, int* step,

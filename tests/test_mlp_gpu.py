@@ -95,3 +95,18 @@ def test_mlp_train_step_replays_from_a_cuda_graph():
     torch.cuda.synchronize()
     assert torch.equal(a.weights, b.weights)
     assert int(a.step_count.item()) == int(b.step_count.item()) == 6
+
+
+def test_data_parallel_step_on_one_rank_equals_train_step():
+    from complex_valued_quadratic_phase_gaussian_b200.mlp import TileMLP
+    M = 384
+    X, T, wout = _batch(M, 13)
+    Xg, Tg, wg = (torch.from_numpy(a).cuda() for a in (X, T, wout))
+    a = TileMLP(M, weights=torch.from_numpy(om.init_weights(D, H, O, seed=8)))
+    b = TileMLP(M, weights=torch.from_numpy(om.init_weights(D, H, O, seed=8)))
+    for _ in range(3):
+        la = a.train_step(Xg, Tg, wg).clone()
+        lb = b.data_parallel_step(Xg, Tg, wg)
+    torch.cuda.synchronize()
+    assert torch.equal(a.weights, b.weights) and torch.equal(a.adam, b.adam)
+    assert abs(float(la.item()) - float(lb.item())) <= 1e-6 * abs(float(la.item()))
