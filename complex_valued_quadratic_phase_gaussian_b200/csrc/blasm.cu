@@ -195,8 +195,10 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_adj_kernel(Blas
             [=](int, int e) {
                 const int x = e - col0;
                 if (x < 0 || x >= ow) return make_float2(0.f, 0.f);
+                // both loads issued together (the gate on |V|^2 only selects afterwards)
                 const float2 v = __ldg(&vv[x]);
-                const float g = (v.x * v.x + v.y * v.y <= 1.0f) ? 2.0f * __ldg(&gp[x]) : 0.0f;
+                const float gpx = __ldg(&gp[x]);
+                const float g = (v.x * v.x + v.y * v.y <= 1.0f) ? 2.0f * gpx : 0.0f;
                 return make_float2(g * v.x, g * v.y);
             },
             sm, sm + ld, ld, 0, d.row, false);
