@@ -440,7 +440,7 @@ static bool column_split(const FftPlan& plan, ColSplit* cs, int radix_hint) {
     int rmin = plan.n;
     for (int p = 0; p < plan.npass; p++) rmin = std::min(rmin, (int)((plan.code >> (5 * p)) & 31ull));
     cs->ntw = plan.n / rmin;
-    if (((size_t)2 * fft_ld(plan.n) + cs->ntw) * sizeof(float2) + (size_t)plan.n * sizeof(float) > kSmemMax)
+    if (((size_t)2 * fft_ldT<kColPad>(plan.n) + cs->ntw) * sizeof(float2) + (size_t)plan.n * sizeof(float) > kSmemMax)
         return false;
     cs->rl = (int)((plan.code >> (5 * best)) & 31ull);
     cs->mb = best_mb;

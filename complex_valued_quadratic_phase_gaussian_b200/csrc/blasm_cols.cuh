@@ -8,6 +8,7 @@ namespace cvqpg {
 
 constexpr int kRowThreads = 256;
 constexpr int kColThreads = 256;
+constexpr int kColPad = 4;  // shared-memory padding shift of the register-spectrum column kernels
 
 // ---------------------------------------------------------------------------
 // device helpers
@@ -104,7 +105,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
                                                                          const float2* __restrict__ A,
                                                                          float2* __restrict__ B) {
     extern __shared__ float2 sm[];
-    const int NH = d.NH, NW = d.NW, ld = fft_ld(NH);
+    const int NH = d.NH, NW = d.NW, ld = fft_ldT<kColPad>(NH);
     float2* b0 = sm;
     float2* b1 = sm + ld;
     float2* tw = sm + 2 * ld;
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
     const int c = blockIdx.x / NW, kx = blockIdx.x - c * NW;
     const int y0 = (NH >> 1) - (d.pH >> 1), pH = d.pH;
     const float2* src = A + (size_t)c * pH * NW + kx;
-    float2* buf = fft_run_passes(
+    float2* buf = fft_run_passes<kColPad>(
         [=](int, int e) {
             const int y = e - y0;
             return (y < 0 || y >= pH) ? make_float2(0.f, 0.f) : __ldg(&src[(size_t)y * NW]);
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
         if (j < nbL) {
             float2 v[RL];
 #pragma unroll
-            for (int r = 0; r < RL; r++) v[r] = buf[fft_pad(j + r * nbL)];
+            for (int r = 0; r < RL; r++) v[r] = buf[fft_padT<kColPad>(j + r * nbL)];
             apply_twiddles<RL>(v, tw[j]);
             dft<RL>(v, false);
 #pragma unroll
@@ -165,12 +166,12 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
                 }
                 dft<RL>(v, true);
 #pragma unroll
-                for (int r = 0; r < RL; r++) b0[fft_pad(j * RL + r)] = v[r];
+                for (int r = 0; r < RL; r++) b0[fft_padT<kColPad>(j * RL + r)] = v[r];
             }
         }
         __syncthreads();
         float2* dst = B + (size_t)pc * oh * NW + kx;
-        fft_run_passes_to([b0](int, int e) { return b0[fft_pad(e)]; },
+        fft_run_passes_to<kColPad>([b0](int, int e) { return b0[fft_padT<kColPad>(e)]; },
                           [=](int, int a, float2 v) {
                               const int y = a - row0;
                               if ((unsigned)y < (unsigned)oh) dst[(size_t)y * NW] = v;
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
                                                                          const float2* __restrict__ Bt,
                                                                          float2* __restrict__ Ab) {
     extern __shared__ float2 sm[];
-    const int NH = d.NH, NW = d.NW, ld = fft_ld(NH);
+    const int NH = d.NH, NW = d.NW, ld = fft_ldT<kColPad>(NH);
     float2* b0 = sm;
     float2* b1 = sm + ld;
     float2* tw = sm + 2 * ld;
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
     for (int p = 0; p < d.P; p++) {
         const int pc = p * d.C + c;
         const float2* src = Bt + (size_t)pc * oh * NW + kx;
-        float2* buf = fft_run_passes(
+        float2* buf = fft_run_passes<kColPad>(
             [=](int, int e) {
                 const int y = e - row0;
                 return (y < 0 || y >= oh) ? make_float2(0.f, 0.f) : __ldg(&src[(size_t)y * NW]);
@@ -229,7 +230,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
             if (j < nbL) {
                 float2 v[RL];
 #pragma unroll
-                for (int r = 0; r < RL; r++) v[r] = buf[fft_pad(j + r * nbL)];
+                for (int r = 0; r < RL; r++) v[r] = buf[fft_padT<kColPad>(j + r * nbL)];
                 apply_twiddles<RL>(v, tw[j]);
                 dft<RL>(v, false);
                 if (col_ok) {
@@ -255,14 +256,14 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
             for (int r = 0; r < RL; r++) v[r] = acc[b][r];
             dft<RL>(v, true);
 #pragma unroll
-            for (int r = 0; r < RL; r++) b0[fft_pad(j * RL + r)] = v[r];
+            for (int r = 0; r < RL; r++) b0[fft_padT<kColPad>(j * RL + r)] = v[r];
         }
     }
     __syncthreads();
     const int in_h = d.input_mode == 0 ? d.H : d.pH;
     const int r0 = (NH >> 1) - (in_h >> 1);
     float2* dst = Ab + (size_t)c * in_h * NW + kx;
-    fft_run_passes_to([b0](int, int e) { return b0[fft_pad(e)]; },
+    fft_run_passes_to<kColPad>([b0](int, int e) { return b0[fft_padT<kColPad>(e)]; },
                       [=](int, int a, float2 v) {
                           const int y = a - r0;
                           if ((unsigned)y < (unsigned)in_h) dst[(size_t)y * NW] = v;
@@ -290,7 +291,7 @@ void launch_cols_reg_r16(bool adjoint, const BlasmDev& d, const ColSplit& cs, co
 #define CVQPG_DEFINE_COLS_REG(RL)                                                                                  \
     void launch_cols_reg_r##RL(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out, \
                                cudaStream_t s) {                                                                   \
-        const size_t sm = ((size_t)2 * fft_ld(d.NH) + cs.ntw) * sizeof(float2) + (size_t)d.NH * sizeof(float);                                              \
+        const size_t sm = ((size_t)2 * fft_ldT<kColPad>(d.NH) + cs.ntw) * sizeof(float2) + (size_t)d.NH * sizeof(float);                                              \
         if (!adjoint) {                                                                                            \
             if (cs.mb == 1) {                                                                                      \
                 cudaFuncSetAttribute(blasm_cols_fwd_reg_kernel<RL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, \

@@ -30,8 +30,15 @@ struct FftPlan {
     const float2* tw;         // device table W_n^m = exp(-2 pi i m / n), m in [0, n)
 };
 
-__host__ __device__ __forceinline__ int fft_pad(int i) { return i + (i >> 5); }
-__host__ __device__ __forceinline__ int fft_ld(int n) { return fft_pad(n - 1) + 2; }
+// Padded index: one spare slot every 2^PS elements (PS = 5 by default; the
+// column kernels use 4, which also keeps the stride-16 stores of a first
+// radix-16 pass on distinct banks).
+template <int PS = 5>
+__host__ __device__ __forceinline__ int fft_padT(int i) { return i + (i >> PS); }
+template <int PS = 5>
+__host__ __device__ __forceinline__ int fft_ldT(int n) { return fft_padT<PS>(n - 1) + 2; }
+__host__ __device__ __forceinline__ int fft_pad(int i) { return fft_padT<5>(i); }
+__host__ __device__ __forceinline__ int fft_ld(int n) { return fft_ldT<5>(n); }
 
 // ---------------------------------------------------------------------------
 // small DFTs on registers
@@ -159,11 +166,13 @@ __device__ __forceinline__ void split_index(int j, int Ns, float inv_ns, int& q,
 // write of the kept elements). Each thread holds a single butterfly at a time,
 // so the register footprint is one radix. `tw` may point to shared or global memory.
 // ---------------------------------------------------------------------------
-struct SmemSink {
+template <int PS = 5>
+struct SmemSinkT {
     float2* out;
     int ld;
-    __device__ __forceinline__ void operator()(int t, int a, float2 v) const { out[t * ld + fft_pad(a)] = v; }
+    __device__ __forceinline__ void operator()(int t, int a, float2 v) const { out[t * ld + fft_padT<PS>(a)] = v; }
 };
+using SmemSink = SmemSinkT<5>;
 
 template <int R, typename Src, typename Sink>
 __device__ __forceinline__ void fft_pass(Src src, Sink sink, int tshift, int n, int Ns, const float2* tw, bool inv) {
@@ -215,7 +224,7 @@ __device__ __forceinline__ void fft_pass_dispatch(int R, Src src, Sink sink, int
 // ping-pong between the shared buffers a and b; the last pass stores through
 // `last` instead. The caller must synchronise before `first` reads shared data
 // written earlier; ends with a barrier.
-template <typename First, typename Last>
+template <int PS = 5, typename First, typename Last>
 __device__ __forceinline__ void fft_run_passes_to(First first, Last last, float2* a, float2* b, int ld, int tshift,
                                                   int n, unsigned long long code, int npass, int Ns0,
                                                   const float2* tw, bool inv) {
@@ -225,16 +234,16 @@ __device__ __forceinline__ void fft_run_passes_to(First first, Last last, float2
         fft_pass_dispatch(R, first, last, tshift, n, Ns, tw, inv);
         return;
     }
-    fft_pass_dispatch(R, first, SmemSink{a, ld}, tshift, n, Ns, tw, inv);
+    fft_pass_dispatch(R, first, SmemSinkT<PS>{a, ld}, tshift, n, Ns, tw, inv);
     Ns *= R;
     float2* cur = a;
     float2* nxt = b;
     for (int p = 1; p < npass; p++) {
         R = (int)((code >> (5 * p)) & 31ull);
         const float2* in = cur;
-        auto src = [in, ld](int t, int e) { return in[t * ld + fft_pad(e)]; };
+        auto src = [in, ld](int t, int e) { return in[t * ld + fft_padT<PS>(e)]; };
         if (p + 1 < npass)
-            fft_pass_dispatch(R, src, SmemSink{nxt, ld}, tshift, n, Ns, tw, inv);
+            fft_pass_dispatch(R, src, SmemSinkT<PS>{nxt, ld}, tshift, n, Ns, tw, inv);
         else
             fft_pass_dispatch(R, src, last, tshift, n, Ns, tw, inv);
         Ns *= R;
@@ -245,12 +254,12 @@ __device__ __forceinline__ void fft_run_passes_to(First first, Last last, float2
 }
 
 // Same, with the result left in shared memory; returns the buffer holding it.
-template <typename First>
+template <int PS = 5, typename First>
 __device__ __forceinline__ float2* fft_run_passes(First first, float2* a, float2* b, int ld, int tshift, int n,
                                                   unsigned long long code, int npass, int Ns0, const float2* tw,
                                                   bool inv) {
     float2* res = (npass & 1) ? a : b;
-    fft_run_passes_to(first, SmemSink{res, ld}, a, b, ld, tshift, n, code, npass, Ns0, tw, inv);
+    fft_run_passes_to<PS>(first, SmemSinkT<PS>{res, ld}, a, b, ld, tshift, n, code, npass, Ns0, tw, inv);
     return res;
 }
 
