@@ -243,37 +243,37 @@ __global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(const uint32
     hist[threadIdx.x * sort_ctas + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of hist in digit-major order over the active CTA columns.
-__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t* __restrict__ hist,
-                                                         const int32_t* __restrict__ pair_count, int cap,
-                                                         int sort_ctas) {
+// Digit-major exclusive scan of hist in two steps: one CTA per digit scans its
+// row of per-CTA counts in place (coalesced) and records the row total; then one
+// warp-group scans the 256 totals into digit_base. The downsweep adds both.
+__global__ void __launch_bounds__(256) sort_scan_rows_kernel(uint32_t* __restrict__ hist,
+                                                             const int32_t* __restrict__ pair_count, int cap,
+                                                             int sort_ctas, uint32_t* __restrict__ digit_total) {
     const int n = min(pair_count[0], cap);
     const int active = (n + kSortTile - 1) / kSortTile;
-    if (active == 0) return;
-    const int total = 256 * active;
-    const int per = (total + blockDim.x - 1) / blockDim.x;
-    const int e0 = threadIdx.x * per;
-    uint32_t local = 0;
-    for (int i = 0; i < per; i++) {
-        const int e = e0 + i;
-        if (e < total) local += hist[(e / active) * sort_ctas + (e % active)];
+    uint32_t* row = hist + (size_t)blockIdx.x * sort_ctas;
+    uint32_t carry = 0;
+    for (int c0 = 0; c0 < active; c0 += 256) {
+        const int c = c0 + threadIdx.x;
+        const uint32_t v = c < active ? row[c] : 0u;
+        uint32_t total = 0;
+        const uint32_t ex = block_exclusive_scan(v, &total);
+        if (c < active) row[c] = carry + ex;
+        carry += total;
     }
-    uint32_t run = block_exclusive_scan(local, nullptr);
-    for (int i = 0; i < per; i++) {
-        const int e = e0 + i;
-        if (e < total) {
-            uint32_t* p = &hist[(e / active) * sort_ctas + (e % active)];
-            const uint32_t t = *p;
-            *p = run;
-            run += t;
-        }
-    }
+    if (threadIdx.x == 0) digit_total[blockIdx.x] = carry;
+}
+
+__global__ void __launch_bounds__(256) sort_scan_digits_kernel(uint32_t* __restrict__ digit_base) {
+    const uint32_t v = digit_base[threadIdx.x];  // the totals, replaced by their exclusive scan
+    const uint32_t ex = block_exclusive_scan(v, nullptr);
+    digit_base[threadIdx.x] = ex;
 }
 
 __global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const int32_t* __restrict__ pair_count, int cap, int shift,
-    const uint32_t* __restrict__ hist, int sort_ctas) {
+    const uint32_t* __restrict__ hist, const uint32_t* __restrict__ digit_base, int sort_ctas) {
     __shared__ uint32_t wc[kSortWarps][257];  // slot 256 absorbs invalid lanes
     const int n = min(pair_count[0], cap);
     const int base = blockIdx.x * kSortTile;
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
         const int idx = wbase + i * 32 + lane;
         if (idx < n) {
             const uint32_t d = (key[i] >> shift) & 255u;
-            const uint32_t pos = hist[d * sort_ctas + blockIdx.x] + wc[w][d] + rank[i];
+            const uint32_t pos = digit_base[d] + hist[d * sort_ctas + blockIdx.x] + wc[w][d] + rank[i];
             keys_out[pos] = key[i];
             vals_out[pos] = val[i];
         }
@@ -362,6 +362,7 @@ BinWorkspace carve_bin_workspace(Carver& cv, int n, int cap) {
     ws.vals_a = cv.take<uint32_t>(cap > 0 ? cap : 1);
     ws.vals_b = cv.take<uint32_t>(cap > 0 ? cap : 1);
     ws.hist = cv.take<uint32_t>((size_t)256 * ws.sort_ctas);
+    ws.digit_base = cv.take<uint32_t>(256);
     return ws;
 }
 
@@ -392,9 +393,11 @@ void launch_binning(const BinRule& rule, const float* records, const BinWorkspac
                                            : ((p % 2 == 0) ? ws.vals_b : ws.vals_a);
         sort_upsweep_kernel<<<ws.sort_ctas, kSortThreads, 0, stream>>>(kin, pair_count, ws.cap, 8 * p, ws.hist,
                                                                         ws.sort_ctas);
-        sort_scan_kernel<<<1, 1024, 0, stream>>>(ws.hist, pair_count, ws.cap, ws.sort_ctas);
+        sort_scan_rows_kernel<<<256, 256, 0, stream>>>(ws.hist, pair_count, ws.cap, ws.sort_ctas, ws.digit_base);
+        sort_scan_digits_kernel<<<1, 256, 0, stream>>>(ws.digit_base);
         sort_downsweep_kernel<<<ws.sort_ctas, kSortThreads, 0, stream>>>(kin, vin, kout, vout, pair_count, ws.cap,
-                                                                          8 * p, ws.hist, ws.sort_ctas);
+                                                                          8 * p, ws.hist, ws.digit_base,
+                                                                          ws.sort_ctas);
         kin = kout;
         vin = vout;
     }

@@ -24,7 +24,8 @@ struct BinWorkspace {
     uint32_t* keys_b;         // [cap]
     uint32_t* vals_a;         // [cap]
     uint32_t* vals_b;         // [cap]
-    uint32_t* hist;           // [256 * sort_ctas]
+    uint32_t* hist;           // [256 * sort_ctas] per-CTA digit counts, then in-row exclusive offsets
+    uint32_t* digit_base;     // [256] exclusive scan of the digit totals
     int n;
     int cap;
     int sort_ctas;
