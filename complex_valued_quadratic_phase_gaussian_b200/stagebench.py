@@ -5,7 +5,9 @@
 Stages: ``blasm_fwd`` (rows, columns, inverse rows), ``blasm_adj`` (the three
 adjoint passes), ``render`` (binning + splat forward of the drop-in path),
 ``splat_adj`` (the splat adjoint alone, on the lists of one forward call),
-``loss`` (multi-plane loss + SSIM forward and dL/d(pred), with target noise).
+``loss`` (multi-plane loss + SSIM forward and dL/d(pred), with target noise),
+``fit_step`` (whole fused fit iterations of the 1080p RGB fit, default FFT plan),
+``mlp_train`` (training steps of the learned initialiser's MLP, 8192 tiles).
 Only the buffers of that stage are allocated, so the process stays small
 enough for kernel-level profiling. Prints one JSON line with the mean
 milliseconds per call (CUDA events on the launching stream).
@@ -98,6 +100,38 @@ def run(stage, workload, iters=3, warmup=1):
             torch.cuda.synchronize()
             if i >= warmup:
                 times.append(s.elapsed_time(e))
+    elif stage == "fit_step":
+        from .fit import FitConfig, Fitter, synthetic_init
+        from .scenes import multiplane_targets_device, rgb_blobs
+        img, depth = rgb_blobs(H, W, seed=0)
+        targets, q = multiplane_targets_device(img, depth, P)
+        cfg = FitConfig(img_size=(W, H), num_gaussians=w["N"], wavelengths=w["wl"], pixel_pitch=w["pitch"],
+                        num_planes=P, d_val=w["d_val"], volume_depth=w["vd"], num_itrs=2000, seed=0)
+        f = Fitter(cfg, targets, q, init=synthetic_init(cfg, 0))
+        for i in range(warmup + iters):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            f.step()
+            e.record()
+            torch.cuda.synchronize()
+            if i >= warmup:
+                times.append(s.elapsed_time(e))
+    elif stage == "mlp_train":
+        from .mlp import TileMLP
+        M = 8192
+        g = torch.Generator(device="cuda").manual_seed(0)
+        X = torch.rand((M, 1024), device="cuda", generator=g)
+        T = torch.randn((M, 156), device="cuda", generator=g)
+        wo = torch.ones(156, device="cuda")
+        net = TileMLP(M)
+        for i in range(warmup + iters):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            net.train_step(X, T, wo)
+            e.record()
+            torch.cuda.synchronize()
+            if i >= warmup:
+                times.append(s.elapsed_time(e))
     else:
         raise ValueError(stage)
     return {"stage": stage, "workload": workload, "ms": float(np.mean(times)), "iters": iters}
@@ -105,7 +139,7 @@ def run(stage, workload, iters=3, warmup=1):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--stage", default="blasm_fwd", choices=["blasm_fwd", "blasm_adj", "render", "splat_adj", "loss"])
+    ap.add_argument("--stage", default="blasm_fwd", choices=["blasm_fwd", "blasm_adj", "render", "splat_adj", "loss", "fit_step", "mlp_train"])
     ap.add_argument("--workload", default="rgb1080", choices=sorted(WORKLOADS))
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
