@@ -200,13 +200,18 @@ def kernels_per_fit_step(cfg):
     return 1 + binning + 1 + 3 + 2 + 1 + 3 + 1 + 1 + 1 + 1
 
 
-def build_scene(wl, seed, device):
+def build_scene(wl, seed, device, ours=False):
+    """Seeded scene and its multi-plane targets: with this library's target kernel for our arm,
+    with the torch restatement of the reference's target synthesis for the reference arms."""
     from complex_valued_quadratic_phase_gaussian_b200 import scenes
     if len(wl["wl"]) == 3:
         img, depth = scenes.rgb_blobs(wl["H"], wl["W"], seed=seed)
     else:
         img, depth = scenes.grayscale_blobs(wl["H"], wl["W"], seed=seed)
-    targets, q = scenes.multiplane_targets_device(img, depth, wl["P"], device=device)
+    if ours:
+        targets, q = scenes.multiplane_targets_device(img, depth, wl["P"], device=device)
+    else:
+        targets, q = scenes.multiplane_targets(img, depth, wl["P"], device=device)
     return img, depth, targets, q
 
 
@@ -312,7 +317,7 @@ def run_ours(args, wl, dist, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     seed = args.seed + rank
-    _, _, targets, q = build_scene(wl, seed, dev)
+    _, _, targets, q = build_scene(wl, seed, dev, ours=True)
     cfg = fit_config(wl, seed, args.primitive)
     init = synthetic_init(cfg, seed)
     fitter = Fitter(cfg, targets, q, init=init, device=dev)
