@@ -512,131 +512,273 @@ void launch_splat_forward(int channels, const BinRule& rule, const int32_t* rang
 }
 
 // ---------------------------------------------------------------------------
-// splat adjoint: Gaussian-parallel. One CTA per tile; each thread owns one
-// Gaussian of the tile list and walks the tile's 256 pixels in lockstep with
-// its warp, so the per-pixel dL/dU reads are shared-memory broadcasts and the
-// per-Gaussian sums stay in registers: no cross-lane reduction, and one atomic
-// per parameter per (Gaussian, tile). The per-pixel terms are recomputed, not
-// stored (same formulas as cuda/backward.cu:101-147, including both paths of
-// dL/dmahal).
+// splat adjoint: balanced over the active (Gaussian, pixel) pairs of a tile.
+// One CTA per tile. For a batch of list entries the CTA first computes, per
+// entry and tile row, the span of columns where the Mahalanobis distance is
+// under the cut (a quadratic in x, solved with a small outward margin; the
+// exact per-pixel test still applies), and a prefix over the entries' active
+// pixel counts. The flattened list of active pairs is then split into equal
+// contiguous ranges, one per thread, so every lane evaluates a live pixel on
+// every step instead of idling where its Gaussian does not reach. A thread's
+// per-Gaussian sums stay in registers until its range leaves that Gaussian,
+// then go to shared per-entry accumulators; one global atomic per parameter
+// per (Gaussian, tile) follows. Per-pixel terms are recomputed (same formulas
+// as cuda/backward.cu:101-147, including both paths of dL/dmahal).
 // ---------------------------------------------------------------------------
-constexpr int kBwdThreads = 64;
+constexpr int kBwdThreads = 128;
+constexpr int kBwdBatch = 256;  // list entries per batch
+
+// Columns [x0, x0 + n) of tile row `fy` (tile origin tx0, xmax columns) where
+// the Gaussian (mx, my, inverse covariance i00 i01 i11) may be under the cut.
+__device__ __forceinline__ void cut_row_span(float mx, float my, float i00, float i01, float i11, float fy, int tx0,
+                                             int xmax, int* x0, int* n) {
+    const float cut = kMahalCut * 1.001f;
+    const float dy = my - fy;
+    // i00 dx^2 + 2 i01 dy dx + i11 dy^2 < cut, dx = mx - x
+    const float q = fmaf(i01 * dy, i01 * dy, -i00 * fmaf(i11 * dy, dy, -cut));
+    if (!(i00 > 0.0f) || !(q < 3.0e38f) || !(i00 < 3.0e38f)) {  // degenerate: scan the whole row
+        *x0 = 0;
+        *n = xmax;
+        return;
+    }
+    if (q < 0.0f) {
+        *x0 = 0;
+        *n = 0;
+        return;
+    }
+    const float centre = mx + i01 * dy / i00 - (float)tx0;  // x of the minimum, tile-relative
+    const float hw = sqrtf(q) / i00 + 1.0e-3f;
+    const float lo = fmaxf(ceilf(centre - hw), 0.0f);
+    const float hi = fminf(floorf(centre + hw), (float)(xmax - 1));
+    if (!(hi >= lo)) {
+        *x0 = 0;
+        *n = 0;
+        return;
+    }
+    *x0 = (int)lo;
+    *n = (int)hi - (int)lo + 1;
+}
 
 template <int C, bool ISO>
 __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     BinRule rule, const int32_t* __restrict__ ranges, const int32_t* __restrict__ point_list,
     const float4* __restrict__ rec, const float* __restrict__ k, float dxy2, const float2* __restrict__ grad, int W,
     int H, int gx, SplatGrads out) {
-    __shared__ float2 s_g[kTilePixels][C];
+    constexpr int NA = 8 + 2 * C;  // dmx dmy d00 d01 d11 dop dcv dar dcol[C] dph[C]
+    constexpr int kWarps = kBwdThreads / 32;
+    constexpr int kPer = kBwdBatch / kBwdThreads;  // entries per thread in the span pass
+    __shared__ float2 s_g[C][kTilePixels];
+    __shared__ uint8_t s_x0[kBwdBatch][kTile];
+    __shared__ uint8_t s_n[kBwdBatch][kTile];
+    __shared__ int s_off[kBwdBatch + 1];
+    __shared__ float s_acc[NA][kBwdBatch];
+    __shared__ int s_wsum[kWarps];
+    static_assert(kBwdBatch % kBwdThreads == 0, "whole entries per thread");
+
     const int tile = blockIdx.x;
     const int2 range = reinterpret_cast<const int2*>(ranges)[list_of_tile(rule, tile % gx, tile / gx)];
     if (range.y <= range.x) return;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     const int tx0 = (tile % gx) * kTile, ty0 = (tile / gx) * kTile;
-    for (int p = threadIdx.x; p < kTilePixels; p += kBwdThreads) {
+    for (int p = t; p < kTilePixels; p += kBwdThreads) {
         const int px = tx0 + (p & 15), py = ty0 + (p >> 4);
         const bool inside = px < W && py < H;
 #pragma unroll
         for (int c = 0; c < C; c++)
-            s_g[p][c] = inside ? grad[(size_t)c * H * W + (size_t)py * W + px] : make_float2(0.0f, 0.0f);
+            s_g[c][p] = inside ? grad[(size_t)c * H * W + (size_t)py * W + px] : make_float2(0.0f, 0.0f);
     }
-    __syncthreads();
     const int xmax = min(kTile, W - tx0), ymax = min(kTile, H - ty0);
 
     float kc[C];
 #pragma unroll
     for (int c = 0; c < C; c++) kc[c] = k[c];
 
-    for (int b = range.x; b < range.y; b += kBwdThreads) {
-        const int i = b + threadIdx.x;
-        if (i >= range.y) break;
-        const int g = point_list[i];
-        const float4 r0 = __ldg(&rec[(size_t)g * 4 + 0]);
-        const float4 r1 = __ldg(&rec[(size_t)g * 4 + 1]);
-        const float4 r2 = __ldg(&rec[(size_t)g * 4 + 2]);
-        const float4 r3 = __ldg(&rec[(size_t)g * 4 + 3]);
-        const float mx = r0.x, my = r0.y, i00 = r0.z, i01 = r0.w, i11 = r1.x;
-        const float opac = r1.y, curv = r1.z, ar = r1.w;
-        float col[C], ph[C];
-        if (C == 1) {
-            col[0] = r2.x;
-            ph[0] = r2.y;
-        } else {
-            col[0] = r2.x;
-            col[C > 1 ? 1 : 0] = r2.y;
-            col[C > 2 ? 2 : 0] = r2.z;
-            ph[0] = r2.w;
-            ph[C > 1 ? 1 : 0] = r3.x;
-            ph[C > 2 ? 2 : 0] = r3.y;
+    for (int b0 = range.x; b0 < range.y; b0 += kBwdBatch) {
+        const int nb = min(kBwdBatch, range.y - b0);
+        // 1. spans and active counts; thread t owns entries kPer*t .. kPer*t + kPer-1
+        int cnt[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; u++) {
+            const int e = kPer * t + u;
+            cnt[u] = 0;
+            if (e < nb) {
+                const int g = point_list[b0 + e];
+                const float4 r0 = __ldg(&rec[(size_t)g * 4 + 0]);
+                const float i11 = __ldg(&rec[(size_t)g * 4 + 1]).x;
+                for (int yy = 0; yy < kTile; yy++) {
+                    int x0 = 0, n = 0;
+                    if (yy < ymax) cut_row_span(r0.x, r0.y, r0.z, r0.w, i11, (float)(ty0 + yy), tx0, xmax, &x0, &n);
+                    s_x0[e][yy] = (uint8_t)x0;
+                    s_n[e][yy] = (uint8_t)n;
+                    cnt[u] += n;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NA; q++) s_acc[q][e] = 0.0f;
         }
-        const float kb = 0.5f * curv * ar * dxy2;  // dbase/dmahal
+        // 2. exclusive prefix of the counts in entry order
+        int local = 0;
+#pragma unroll
+        for (int u = 0; u < kPer; u++) local += cnt[u];
+        int incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_wsum[wid] = incl;
+        __syncthreads();
+        int base = 0;
+        for (int w = 0; w < wid; w++) base += s_wsum[w];
+        int run = base + incl - local;
+#pragma unroll
+        for (int u = 0; u < kPer; u++) {
+            s_off[kPer * t + u] = run;
+            run += cnt[u];
+        }
+        if (t == kBwdThreads - 1) s_off[kBwdBatch] = run;
+        __syncthreads();
 
-        float dmx = 0.f, dmy = 0.f, d00 = 0.f, d01 = 0.f, d11 = 0.f, dop = 0.f, dcv = 0.f, dar = 0.f;
-        float dcol[C], dph[C];
-#pragma unroll
-        for (int c = 0; c < C; c++) {
-            dcol[c] = 0.f;
-            dph[c] = 0.f;
-        }
-        for (int yy = 0; yy < ymax; yy++) {
-            const float dy = my - (float)(ty0 + yy);
-            for (int xx = 0; xx < xmax; xx++) {
-                const float dx = mx - (float)(tx0 + xx);
-                const float mahal = dx * (i00 * dx + i01 * dy) + dy * (i01 * dx + i11 * dy);
-                if (mahal >= kMahalCut) continue;
-                const float raw_power = -0.5f * mahal;
-                const float G = __expf(fmaxf(raw_power, -50.0f));
-                const float alpha = opac * G;
-                const float d2 = dx * dx + dy * dy;
-                const float base = ISO ? 0.5f * curv * d2 * dxy2 : 0.5f * curv * mahal * ar * dxy2;
-                const int p = yy * kTile + xx;
-                float S_alpha = 0.f, S_base = 0.f;
-#pragma unroll
-                for (int c = 0; c < C; c++) {
-                    float s, co;
-                    sincos_reduced(ph[c] + kc[c] * base, &s, &co);
-                    const float2 gp = s_g[p][c];
-                    const float proj_c = gp.x * co + gp.y * s;
-                    const float proj_s = -gp.x * s + gp.y * co;
-                    const float aph = col[c] * alpha * proj_s;
-                    dcol[c] = fmaf(alpha, proj_c, dcol[c]);
-                    dph[c] += aph;
-                    S_alpha = fmaf(col[c], proj_c, S_alpha);
-                    S_base = fmaf(kc[c], aph, S_base);
-                }
-                const float dpow = (raw_power >= -50.0f) ? -0.5f : 0.0f;
-                float dmahal;
-                if (ISO) {
-                    // the phase reaches the means directly: dbase/dmu = c dxy2 (mu - r)
-                    dmahal = S_alpha * opac * G * dpow;
-                    dcv = fmaf(S_base, 0.5f * d2 * dxy2, dcv);
-                    dmx = fmaf(S_base * curv * dxy2, dx, dmx);
-                    dmy = fmaf(S_base * curv * dxy2, dy, dmy);
+        // 3. this thread's contiguous share of the active pairs
+        const int total = s_off[kBwdBatch];
+        const int lo = (int)(((long long)total * t) / kBwdThreads);
+        const int hi = (int)(((long long)total * (t + 1)) / kBwdThreads);
+        if (lo < hi) {
+            int e = 0;  // last entry starting at or before lo
+            for (int step = kBwdBatch / 2; step > 0; step >>= 1)
+                if (e + step < nb && s_off[e + step] <= lo) e += step;
+            int r = 0, o = lo - s_off[e];
+            while (o >= (int)s_n[e][r]) {
+                o -= s_n[e][r];
+                r++;
+            }
+            int x = s_x0[e][r] + o, rem = s_n[e][r] - o;
+
+            int g = point_list[b0 + e];
+            float mx, my, i00, i01, i11, opac, curv, ar, kb, har, hcv, col[C], ph[C];
+            auto load = [&](int gg) {
+                const float4 r0 = __ldg(&rec[(size_t)gg * 4 + 0]);
+                const float4 r1 = __ldg(&rec[(size_t)gg * 4 + 1]);
+                const float4 r2 = __ldg(&rec[(size_t)gg * 4 + 2]);
+                mx = r0.x, my = r0.y, i00 = r0.z, i01 = r0.w, i11 = r1.x;
+                opac = r1.y, curv = r1.z, ar = r1.w;
+                kb = 0.5f * curv * ar * dxy2;  // dbase/dmahal
+                har = 0.5f * ar * dxy2;
+                hcv = 0.5f * curv * dxy2;
+                if (C == 1) {
+                    col[0] = r2.x;
+                    ph[0] = r2.y;
                 } else {
-                    dmahal = S_alpha * opac * G * dpow + S_base * kb;
-                    dcv = fmaf(S_base, 0.5f * mahal * ar * dxy2, dcv);
-                    dar = fmaf(S_base, 0.5f * curv * mahal * dxy2, dar);
+                    const float4 r3 = __ldg(&rec[(size_t)gg * 4 + 3]);
+                    col[0] = r2.x;
+                    col[C > 1 ? 1 : 0] = r2.y;
+                    col[C > 2 ? 2 : 0] = r2.z;
+                    ph[0] = r2.w;
+                    ph[C > 1 ? 1 : 0] = r3.x;
+                    ph[C > 2 ? 2 : 0] = r3.y;
                 }
-                d00 = fmaf(dmahal, dx * dx, d00);
-                d01 = fmaf(dmahal, 2.0f * dx * dy, d01);
-                d11 = fmaf(dmahal, dy * dy, d11);
-                dmx = fmaf(dmahal, 2.0f * (i00 * dx + i01 * dy), dmx);
-                dmy = fmaf(dmahal, 2.0f * (i11 * dy + i01 * dx), dmy);
-                dop = fmaf(S_alpha, G, dop);
+            };
+            load(g);
+            float acc[NA];
+#pragma unroll
+            for (int q = 0; q < NA; q++) acc[q] = 0.0f;
+            auto flush = [&](int ee) {
+#pragma unroll
+                for (int q = 0; q < NA; q++) {
+                    if (acc[q] != 0.0f) atomicAdd(&s_acc[q][ee], acc[q]);
+                    acc[q] = 0.0f;
+                }
+            };
+
+            for (int it = lo; it < hi; it++) {
+                const float dx = mx - (float)(tx0 + x);
+                const float dy = my - (float)(ty0 + r);
+                const float mahal = dx * (i00 * dx + i01 * dy) + dy * (i01 * dx + i11 * dy);
+                if (mahal < kMahalCut) {
+                    const float raw_power = -0.5f * mahal;
+                    const float G = __expf(fmaxf(raw_power, -50.0f));
+                    const float alpha = opac * G;
+                    const float d2 = dx * dx + dy * dy;
+                    const float base = ISO ? 0.5f * curv * d2 * dxy2 : 0.5f * curv * mahal * ar * dxy2;
+                    const int p = r * kTile + x;
+                    float S_alpha = 0.f, S_base = 0.f;
+#pragma unroll
+                    for (int c = 0; c < C; c++) {
+                        float s, co;
+                        sincos_reduced(ph[c] + kc[c] * base, &s, &co);
+                        const float2 gp = s_g[c][p];
+                        const float proj_c = gp.x * co + gp.y * s;
+                        const float proj_s = -gp.x * s + gp.y * co;
+                        const float aph = col[c] * alpha * proj_s;
+                        acc[8 + c] = fmaf(alpha, proj_c, acc[8 + c]);
+                        acc[8 + C + c] += aph;
+                        S_alpha = fmaf(col[c], proj_c, S_alpha);
+                        S_base = fmaf(kc[c], aph, S_base);
+                    }
+                    const float dpow = (raw_power >= -50.0f) ? -0.5f : 0.0f;
+                    float dmahal;
+                    if (ISO) {
+                        // the phase reaches the means directly: dbase/dmu = c dxy2 (mu - r)
+                        dmahal = S_alpha * opac * G * dpow;
+                        acc[6] = fmaf(S_base, 0.5f * d2 * dxy2, acc[6]);
+                        acc[0] = fmaf(S_base * curv * dxy2, dx, acc[0]);
+                        acc[1] = fmaf(S_base * curv * dxy2, dy, acc[1]);
+                    } else {
+                        dmahal = S_alpha * opac * G * dpow + S_base * kb;
+                        acc[6] = fmaf(S_base * mahal, har, acc[6]);
+                        acc[7] = fmaf(S_base * mahal, hcv, acc[7]);
+                    }
+                    acc[2] = fmaf(dmahal, dx * dx, acc[2]);
+                    acc[3] = fmaf(dmahal, 2.0f * dx * dy, acc[3]);
+                    acc[4] = fmaf(dmahal, dy * dy, acc[4]);
+                    acc[0] = fmaf(dmahal, 2.0f * (i00 * dx + i01 * dy), acc[0]);
+                    acc[1] = fmaf(dmahal, 2.0f * (i11 * dy + i01 * dx), acc[1]);
+                    acc[5] = fmaf(S_alpha, G, acc[5]);
+                }
+                // advance to the next active pixel of this entry, or to the next entry
+                x++;
+                if (--rem == 0) {
+                    do {
+                        r++;
+                    } while (r < kTile && s_n[e][r] == 0);
+                    if (r == kTile) {
+                        flush(e);
+                        if (it + 1 >= hi) break;
+                        e++;
+                        while (e + 1 < nb && s_off[e + 1] == s_off[e]) e++;  // skip entries with no active pixel
+                        g = point_list[b0 + e];
+                        load(g);
+                        r = 0;
+                        while (r < kTile - 1 && s_n[e][r] == 0) r++;
+                    }
+                    x = s_x0[e][r];
+                    rem = s_n[e][r];
+                }
+            }
+            flush(e);  // no-op when the range ended on an entry boundary (sums already cleared)
+        }
+        __syncthreads();
+        // 4. one global atomic per parameter per (Gaussian, tile)
+        for (int e = t; e < nb; e += kBwdThreads) {
+            const int g = point_list[b0 + e];
+            float v[NA];
+#pragma unroll
+            for (int q = 0; q < NA; q++) v[q] = s_acc[q][e];
+            if (v[0] != 0.f) atomicAdd(&out.d_means[2 * g], v[0]);
+            if (v[1] != 0.f) atomicAdd(&out.d_means[2 * g + 1], v[1]);
+            if (v[2] != 0.f) atomicAdd(&out.d_inv[3 * g], v[2]);
+            if (v[3] != 0.f) atomicAdd(&out.d_inv[3 * g + 1], v[3]);
+            if (v[4] != 0.f) atomicAdd(&out.d_inv[3 * g + 2], v[4]);
+            if (v[5] != 0.f) atomicAdd(&out.d_op[g], v[5]);
+            if (v[6] != 0.f) atomicAdd(&out.d_cv[g], v[6]);
+            if (v[7] != 0.f) atomicAdd(&out.d_ar[g], v[7]);
+#pragma unroll
+            for (int c = 0; c < C; c++) {
+                if (v[8 + c] != 0.f) atomicAdd(&out.d_col[g * C + c], v[8 + c]);
+                if (v[8 + C + c] != 0.f) atomicAdd(&out.d_ph[g * C + c], v[8 + C + c]);
             }
         }
-        if (dmx != 0.f) atomicAdd(&out.d_means[2 * g], dmx);
-        if (dmy != 0.f) atomicAdd(&out.d_means[2 * g + 1], dmy);
-        if (d00 != 0.f) atomicAdd(&out.d_inv[3 * g], d00);
-        if (d01 != 0.f) atomicAdd(&out.d_inv[3 * g + 1], d01);
-        if (d11 != 0.f) atomicAdd(&out.d_inv[3 * g + 2], d11);
-        if (dop != 0.f) atomicAdd(&out.d_op[g], dop);
-        if (dcv != 0.f) atomicAdd(&out.d_cv[g], dcv);
-        if (dar != 0.f) atomicAdd(&out.d_ar[g], dar);
-#pragma unroll
-        for (int c = 0; c < C; c++) {
-            if (dcol[c] != 0.f) atomicAdd(&out.d_col[g * C + c], dcol[c]);
-            if (dph[c] != 0.f) atomicAdd(&out.d_ph[g * C + c], dph[c]);
-        }
+        __syncthreads();
     }
 }
 
