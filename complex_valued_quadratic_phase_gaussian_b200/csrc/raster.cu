@@ -568,8 +568,9 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     constexpr int kWarps = kBwdThreads / 32;
     constexpr int kPer = kBwdBatch / kBwdThreads;  // entries per thread in the span pass
     __shared__ float2 s_g[C][kTilePixels];
-    __shared__ uint8_t s_x0[kBwdBatch][kTile];
-    __shared__ uint8_t s_n[kBwdBatch][kTile];
+    // non-empty rows of each entry, in order: y | x0 << 4 | (n - 1) << 8
+    __shared__ uint16_t s_rows[kBwdBatch][kTile];
+    __shared__ uint8_t s_nr[kBwdBatch];
     __shared__ int s_off[kBwdBatch + 1];
     __shared__ float s_acc[NA][kBwdBatch];
     __shared__ int s_wsum[kWarps];
@@ -601,18 +602,21 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
         for (int u = 0; u < kPer; u++) {
             const int e = kPer * t + u;
             cnt[u] = 0;
+            int nr = 0;
             if (e < nb) {
                 const int g = point_list[b0 + e];
                 const float4 r0 = __ldg(&rec[(size_t)g * 4 + 0]);
                 const float i11 = __ldg(&rec[(size_t)g * 4 + 1]).x;
-                for (int yy = 0; yy < kTile; yy++) {
-                    int x0 = 0, n = 0;
-                    if (yy < ymax) cut_row_span(r0.x, r0.y, r0.z, r0.w, i11, (float)(ty0 + yy), tx0, xmax, &x0, &n);
-                    s_x0[e][yy] = (uint8_t)x0;
-                    s_n[e][yy] = (uint8_t)n;
-                    cnt[u] += n;
+                for (int yy = 0; yy < ymax; yy++) {
+                    int x0, n;
+                    cut_row_span(r0.x, r0.y, r0.z, r0.w, i11, (float)(ty0 + yy), tx0, xmax, &x0, &n);
+                    if (n > 0) {
+                        s_rows[e][nr++] = (uint16_t)(yy | (x0 << 4) | ((n - 1) << 8));
+                        cnt[u] += n;
+                    }
                 }
             }
+            s_nr[e] = (uint8_t)nr;
 #pragma unroll
             for (int q = 0; q < NA; q++) s_acc[q][e] = 0.0f;
         }
@@ -647,12 +651,14 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
             int e = 0;  // last entry starting at or before lo
             for (int step = kBwdBatch / 2; step > 0; step >>= 1)
                 if (e + step < nb && s_off[e + step] <= lo) e += step;
-            int r = 0, o = lo - s_off[e];
-            while (o >= (int)s_n[e][r]) {
-                o -= s_n[e][r];
-                r++;
+            int k = 0, o = lo - s_off[e];
+            int w = s_rows[e][0];
+            while (o > (w >> 8)) {  // o >= row length
+                o -= (w >> 8) + 1;
+                w = s_rows[e][++k];
             }
-            int x = s_x0[e][r] + o, rem = s_n[e][r] - o;
+            int nr = s_nr[e];
+            int r = w & 15, x = ((w >> 4) & 15) + o, rem = (w >> 8) + 1 - o;
 
             int g = point_list[b0 + e];
             float mx, my, i00, i01, i11, opac, curv, ar, kb, har, hcv, col[C], ph[C];
@@ -738,21 +744,20 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
                 // advance to the next active pixel of this entry, or to the next entry
                 x++;
                 if (--rem == 0) {
-                    do {
-                        r++;
-                    } while (r < kTile && s_n[e][r] == 0);
-                    if (r == kTile) {
+                    if (++k == nr) {
                         flush(e);
                         if (it + 1 >= hi) break;
                         e++;
                         while (e + 1 < nb && s_off[e + 1] == s_off[e]) e++;  // skip entries with no active pixel
                         g = point_list[b0 + e];
                         load(g);
-                        r = 0;
-                        while (r < kTile - 1 && s_n[e][r] == 0) r++;
+                        nr = s_nr[e];
+                        k = 0;
                     }
-                    x = s_x0[e][r];
-                    rem = s_n[e][r];
+                    w = s_rows[e][k];
+                    r = w & 15;
+                    x = (w >> 4) & 15;
+                    rem = (w >> 8) + 1;
                 }
             }
             flush(e);  // no-op when the range ended on an entry boundary (sums already cleared)
