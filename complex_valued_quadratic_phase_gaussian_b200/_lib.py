@@ -44,6 +44,8 @@ _SIGNATURES = {
     "cvqpg_blasm_backward": [_p, _p, _sz, _p, _p, _p, _p, _sz, _p],
     "cvqpg_loss_workspace_size": [_p, _psz],
     "cvqpg_loss_target_range": [_p, _i, _i, _i, _i, _p, _p, _sz, _p],
+    "cvqpg_loss_target_moments_size": [_p, _psz],
+    "cvqpg_loss_target_moments": [_p, _p, _p, _sz, _p],
     "cvqpg_loss_forward_backward": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
     "cvqpg_targets_workspace_size": [_i, _i, _i, _i, _psz],
     "cvqpg_targets_synthesize": [_p, _p, _i, _i, _i, _i, _i, _f, _f, _p, _p, _p, _sz, _p],

@@ -68,6 +68,7 @@ static int fit_dims(const cvqpg_fit_params* q, cvqpg_blasm_params* bp, cvqpg_los
     lp->noise_ratio = q->noise_ratio;
     lp->inject_noise = q->inject_noise;
     lp->seed = q->seed;
+    lp->target_moments = q->target_moments;
     return CVQPG_OK;
 }
 

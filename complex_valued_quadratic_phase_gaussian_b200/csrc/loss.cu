@@ -39,9 +39,12 @@ constexpr int kVSeg = 7;             // vertical moments + SSIM: 42 columns x (4
 constexpr int kTHSeg = 8;            // transposed horizontal: 42 rows x (32 = 4 x 8) columns
 constexpr int kTVSeg = 4;            // transposed vertical: 32 columns x (32 = 8 x 4) rows, one Philox call
 constexpr int kRegionA = 2 * kLH * kSXLd;  // sX, sY; later the three SSIM partial maps
-constexpr int kRegionB = 5 * kLH * kHMLd;  // five moment maps; later the transposed-horizontal maps
+// NM moment maps filtered per call: 5 (pred, target, pred^2, target^2, pred*target), or 3
+// (pred, pred^2, pred*target) when the target moments are precomputed; later the
+// transposed-horizontal maps
+constexpr int region_b(int nm) { return nm * kLH * kHMLd; }
 static_assert(3 * kLM * kHMLd <= kRegionA, "SSIM partial maps must fit in the staging region");
-static_assert(3 * kLM * kTMLd <= kRegionB, "transposed maps must fit in the moment region");
+static_assert(3 * kLM * kTMLd <= region_b(3), "transposed maps must fit in the moment region");
 static_assert((kLM / kVSeg) * kLM <= kLossThreads, "one vertical item per thread");
 static_assert((kLT / kTHSeg) * kLM <= kLossThreads, "one transposed-horizontal item per thread");
 static_assert((kLT / kTVSeg) * kLT == kLossThreads, "one transposed-vertical item per thread");
@@ -54,6 +57,7 @@ __device__ __forceinline__ float ssim_w(int k) {
     return w[k];
 }
 
+template <int NM>
 __global__ void __launch_bounds__(kLossThreads, 3) loss_kernel(LossDev L, const float* __restrict__ pred,
                                                                 const float* __restrict__ target,
                                                                 const uint8_t* __restrict__ depth_plane,
@@ -90,34 +94,41 @@ __global__ void __launch_bounds__(kLossThreads, 3) loss_kernel(LossDev L, const 
     }
     __syncthreads();
 
-    // 2. horizontal filter -> moments x, y, xx, yy, xy on [52][42]; item = (row, 7 columns)
+    // 2. horizontal filter -> moments on [52][42]; item = (row, 7 columns).
+    //    NM = 5: x, y, xx, yy, xy.  NM = 3: x, xx, xy (target moments precomputed).
     for (int item = tid; item < kLH * (kLM / kHSeg); item += kLossThreads) {
         const int r = item % kLH, c0 = (item / kLH) * kHSeg;
-        float acc[5][kHSeg];
+        float acc[NM][kHSeg];
 #pragma unroll
         for (int o = 0; o < kHSeg; o++)
 #pragma unroll
-            for (int m = 0; m < 5; m++) acc[m][o] = 0.f;
+            for (int m = 0; m < NM; m++) acc[m][o] = 0.f;
         const float* px = sX + r * kSXLd + c0;
         const float* py = sY + r * kSXLd + c0;
 #pragma unroll
         for (int k = 0; k < kHSeg + 10; k++) {
             const float x = px[k], y = py[k];
-            const float xx = x * x, yy = y * y, xy = x * y;
+            const float xx = x * x, xy = x * y;
 #pragma unroll
             for (int o = 0; o < kHSeg; o++) {
                 const int t = k - o;
                 if (t < 0 || t > 10) continue;
                 const float w = ssim_w(t);
-                acc[0][o] = fmaf(w, x, acc[0][o]);
-                acc[1][o] = fmaf(w, y, acc[1][o]);
-                acc[2][o] = fmaf(w, xx, acc[2][o]);
-                acc[3][o] = fmaf(w, yy, acc[3][o]);
-                acc[4][o] = fmaf(w, xy, acc[4][o]);
+                if (NM == 5) {
+                    acc[0][o] = fmaf(w, x, acc[0][o]);
+                    acc[1][o] = fmaf(w, y, acc[1][o]);
+                    acc[2][o] = fmaf(w, xx, acc[2][o]);
+                    acc[3 % NM][o] = fmaf(w, y * y, acc[3 % NM][o]);
+                    acc[4 % NM][o] = fmaf(w, xy, acc[4 % NM][o]);
+                } else {
+                    acc[0][o] = fmaf(w, x, acc[0][o]);
+                    acc[1][o] = fmaf(w, xx, acc[1][o]);
+                    acc[2][o] = fmaf(w, xy, acc[2][o]);
+                }
             }
         }
 #pragma unroll
-        for (int m = 0; m < 5; m++)
+        for (int m = 0; m < NM; m++)
 #pragma unroll
             for (int o = 0; o < kHSeg; o++) hM[m * kLH * kHMLd + r * kHMLd + c0 + o] = acc[m][o];
     }
@@ -128,23 +139,23 @@ __global__ void __launch_bounds__(kLossThreads, 3) loss_kernel(LossDev L, const 
     float ssim_sum = 0.f;
     if (tid < kLM * (kLM / kVSeg)) {
         const int jj = tid % kLM, i0 = (tid / kLM) * kVSeg;
-        float acc[5][kVSeg];
+        float acc[NM][kVSeg];
 #pragma unroll
         for (int o = 0; o < kVSeg; o++)
 #pragma unroll
-            for (int m = 0; m < 5; m++) acc[m][o] = 0.f;
+            for (int m = 0; m < NM; m++) acc[m][o] = 0.f;
 #pragma unroll
         for (int k = 0; k < kVSeg + 10; k++) {
-            float v[5];
+            float v[NM];
 #pragma unroll
-            for (int m = 0; m < 5; m++) v[m] = hM[m * kLH * kHMLd + (i0 + k) * kHMLd + jj];
+            for (int m = 0; m < NM; m++) v[m] = hM[m * kLH * kHMLd + (i0 + k) * kHMLd + jj];
 #pragma unroll
             for (int o = 0; o < kVSeg; o++) {
                 const int t = k - o;
                 if (t < 0 || t > 10) continue;
                 const float w = ssim_w(t);
 #pragma unroll
-                for (int m = 0; m < 5; m++) acc[m][o] = fmaf(w, v[m], acc[m][o]);
+                for (int m = 0; m < NM; m++) acc[m][o] = fmaf(w, v[m], acc[m][o]);
             }
         }
         const int mj = x0 - 10 + jj;
@@ -154,8 +165,15 @@ __global__ void __launch_bounds__(kLossThreads, 3) loss_kernel(LossDev L, const 
             const int ii = i0 + o, mi = y0 - 10 + ii;
             float dm = 0.f, dxx = 0.f, dxy = 0.f;
             if (col_ok && (unsigned)mi < (unsigned)(H - 10)) {
-                const float mu1 = acc[0][o], mu2 = acc[1][o];
-                const float s11 = acc[2][o] - mu1 * mu1, s22 = acc[3][o] - mu2 * mu2, s12 = acc[4][o] - mu1 * mu2;
+                float mu1, mu2, exx, eyy, exy;
+                if (NM == 5) {
+                    mu1 = acc[0][o], mu2 = acc[1 % NM][o], exx = acc[2 % NM][o], eyy = acc[3 % NM][o];
+                    exy = acc[4 % NM][o];
+                } else {
+                    const float2 tm = __ldg(&L.tmom[((size_t)pc * (H - 10) + mi) * (W - 10) + mj]);
+                    mu1 = acc[0][o], exx = acc[1][o], exy = acc[2][o], mu2 = tm.x, eyy = tm.y;
+                }
+                const float s11 = exx - mu1 * mu1, s22 = eyy - mu2 * mu2, s12 = exy - mu1 * mu2;
                 const float A1 = 2.f * mu1 * mu2 + C1, A2 = 2.f * s12 + C2;
                 const float B1 = mu1 * mu1 + mu2 * mu2 + C1, B2 = s11 + s22 + C2;
                 const float iB1 = 1.f / B1, iB2 = 1.f / B2;
@@ -407,6 +425,7 @@ int loss_make_dev(const cvqpg_loss_params* q, LossDev* L) {
     L->c2 = (float)((0.03 * 1.0) * (0.03 * 1.0));
     L->inv_n = (float)(1.0 / ((double)L->C * L->H * L->W));
     L->inv_nmap = (float)(1.0 / ((double)L->C * (L->H - 10) * (L->W - 10)));
+    L->tmom = reinterpret_cast<const float2*>(q->target_moments);
     return CVQPG_OK;
 }
 
@@ -415,16 +434,76 @@ size_t loss_partials_floats(const LossDev& L) {
     return (size_t)L.P * L.C * tiles * 3;
 }
 
-static size_t loss_smem() { return (size_t)(kRegionA + kRegionB) * sizeof(float); }
+static size_t loss_smem(int nm) { return (size_t)(kRegionA + region_b(nm)) * sizeof(float); }
+
+// Target moments: one CTA per 32x32 block of map positions of one (plane, channel)
+// image; the same two separable passes and fma order as the loss kernel's.
+constexpr int kTmIn = kLT + 10;  // 42 staged rows / columns
+__global__ void __launch_bounds__(kLossThreads) target_moments_kernel(int H, int W, const float* __restrict__ targets,
+                                                                      float2* __restrict__ mom) {
+    __shared__ float sT[kTmIn][kTmIn + 1];
+    __shared__ float hm[2][kTmIn][kLT + 1];
+    const int MH = H - 10, MW = W - 10;
+    const int tx = (MW + kLT - 1) / kLT, ty = (MH + kLT - 1) / kLT;
+    const int pc = blockIdx.x / (tx * ty), tile = blockIdx.x - pc * tx * ty;
+    const int m0y = (tile / tx) * kLT, m0x = (tile % tx) * kLT;
+    const float* T = targets + (size_t)pc * H * W;
+    for (int i = threadIdx.x; i < kTmIn * kTmIn; i += kLossThreads) {
+        const int r = i / kTmIn, c = i - r * kTmIn;
+        const int y = m0y + r, x = m0x + c;
+        sT[r][c] = (y < H && x < W) ? __ldg(&T[(size_t)y * W + x]) : 0.f;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kTmIn * kLT; i += kLossThreads) {
+        const int r = i / kLT, c = i - r * kLT;
+        float a = 0.f, b = 0.f;
+#pragma unroll
+        for (int t = 0; t <= 10; t++) {
+            const float y = sT[r][c + t];
+            a = fmaf(ssim_w(t), y, a);
+            b = fmaf(ssim_w(t), y * y, b);
+        }
+        hm[0][r][c] = a;
+        hm[1][r][c] = b;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kLT * kLT; i += kLossThreads) {
+        const int r = i / kLT, c = i - r * kLT;
+        float a = 0.f, b = 0.f;
+#pragma unroll
+        for (int t = 0; t <= 10; t++) {
+            a = fmaf(ssim_w(t), hm[0][r + t][c], a);
+            b = fmaf(ssim_w(t), hm[1][r + t][c], b);
+        }
+        const int my = m0y + r, mx = m0x + c;
+        if (my < MH && mx < MW) mom[((size_t)pc * MH + my) * MW + mx] = make_float2(a, b);
+    }
+}
+
+size_t target_moments_bytes(const LossDev& L) {
+    return (size_t)L.P * L.C * (L.H - 10) * (L.W - 10) * sizeof(float2);
+}
+
+void launch_target_moments(const LossDev& L, const float* targets, float2* mom, cudaStream_t stream) {
+    const int tiles = ((L.W - 10 + kLT - 1) / kLT) * ((L.H - 10 + kLT - 1) / kLT);
+    target_moments_kernel<<<L.P * L.C * tiles, kLossThreads, 0, stream>>>(L.H, L.W, targets, mom);
+}
 
 void launch_loss(const LossDev& L, const float* pred, const float* targets, const uint8_t* depth_plane,
                  const float* noise_scale, const int* iteration, float* grad_pred, float* partials, float* out,
                  cudaStream_t stream) {
     const int tiles = ((L.W + kLT - 1) / kLT) * ((L.H + kLT - 1) / kLT);
-    const size_t sm = loss_smem();
-    cudaFuncSetAttribute(loss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    loss_kernel<<<L.P * L.C * tiles, kLossThreads, sm, stream>>>(L, pred, targets, depth_plane, noise_scale,
-                                                                 iteration, grad_pred, partials);
+    if (L.tmom) {
+        const size_t sm = loss_smem(3);
+        cudaFuncSetAttribute(loss_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        loss_kernel<3><<<L.P * L.C * tiles, kLossThreads, sm, stream>>>(L, pred, targets, depth_plane, noise_scale,
+                                                                        iteration, grad_pred, partials);
+    } else {
+        const size_t sm = loss_smem(5);
+        cudaFuncSetAttribute(loss_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        loss_kernel<5><<<L.P * L.C * tiles, kLossThreads, sm, stream>>>(L, pred, targets, depth_plane, noise_scale,
+                                                                        iteration, grad_pred, partials);
+    }
     loss_finalize_kernel<<<1, kFinalThreads, 0, stream>>>(L, partials, out);
 }
 
@@ -461,6 +540,27 @@ extern "C" int cvqpg_loss_target_range(const float* targets, int planes, int cha
     if (workspace_bytes < (size_t)planes * CVQPG_TARGET_RANGE_WORKSPACE_PER_PLANE) return CVQPG_ERR_WORKSPACE;
     launch_target_range(targets, planes, (size_t)channels * height * width, range_out, workspace,
                         (cudaStream_t)stream);
+    return launch_status();
+}
+
+extern "C" int cvqpg_loss_target_moments_size(const cvqpg_loss_params* q, size_t* bytes) {
+    if (!bytes) return CVQPG_ERR_ARG;
+    LossDev L;
+    const int st = loss_make_dev(q, &L);
+    if (st != CVQPG_OK) return st;
+    *bytes = target_moments_bytes(L);
+    return CVQPG_OK;
+}
+
+extern "C" int cvqpg_loss_target_moments(const cvqpg_loss_params* q, const float* targets, float* moments,
+                                         size_t moments_bytes, void* stream) {
+    LossDev L;
+    const int st = loss_make_dev(q, &L);
+    if (st != CVQPG_OK) return st;
+    if (!targets || !moments) return CVQPG_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(moments) % 8 != 0) return CVQPG_ERR_ARG;
+    if (moments_bytes < target_moments_bytes(L)) return CVQPG_ERR_WORKSPACE;
+    launch_target_moments(L, targets, reinterpret_cast<float2*>(moments), (cudaStream_t)stream);
     return launch_status();
 }
 

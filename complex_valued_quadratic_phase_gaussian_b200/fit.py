@@ -45,7 +45,8 @@ class FitParams(ctypes.Structure):
                 ("curv_const", ctypes.c_double), ("lr", ctypes.c_double * 6), ("betas", ctypes.c_double * 3),
                 ("eps", ctypes.c_double), ("weight_decay", ctypes.c_double), ("max_grad_norm", ctypes.c_double),
                 ("loss_weights", ctypes.c_float * 3), ("ssim_weight", ctypes.c_float),
-                ("noise_ratio", ctypes.c_float), ("plan_hint", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
+                ("noise_ratio", ctypes.c_float), ("plan_hint", ctypes.c_int), ("seed", ctypes.c_ulonglong),
+                ("target_moments", ctypes.c_void_p)]
 
 
 @dataclass
@@ -77,6 +78,7 @@ class FitConfig:
     history_len: int = 4096
     plan_hint: int = 0                       # FFT plan of the propagation (autotune.py); 0 = defaults
     autotune: bool = False                   # pick plan_hint by measurement (cached per grid)
+    target_moments: bool = True              # precompute the targets' SSIM window moments once per fit
 
     @property
     def W(self):
@@ -165,6 +167,19 @@ def synthetic_init(cfg, seed=0):
     return {k: torch.from_numpy(np.asarray(v, dtype=np.float32)) for k, v in arr.items()}
 
 
+
+def compute_target_moments(p, targets):
+    """Windowed SSIM moments of fixed targets (cvqpg_loss_target_moments) for a fit's loss."""
+    from .loss import LossParams
+    lib = _lib.lib()
+    P, C, H, W = p.planes, p.channels, p.height, p.width
+    lp = LossParams(C, P, H, W, 1.0, 1.0, 1.0, 0.0, 0.0, 0, 0)
+    nbytes = _lib.size_query(lib.cvqpg_loss_target_moments_size, ctypes.byref(lp))
+    mom = torch.empty(nbytes // 4, dtype=torch.float32, device=targets.device)
+    _lib.check(lib.cvqpg_loss_target_moments(ctypes.byref(lp), _lib.ptr(targets), _lib.ptr(mom), nbytes,
+                                             _lib.stream_of(targets.device)), "cvqpg_loss_target_moments")
+    return mom
+
 class Fitter:
     """Device-resident fit of one hologram with the fused kernels."""
 
@@ -243,6 +258,10 @@ class Fitter:
             _lib.check(lib.cvqpg_loss_target_range(_lib.ptr(self.targets), P, C, H, W, _lib.ptr(self.target_range),
                                                    _lib.ptr(scratch), scratch.numel(), _lib.stream_of(self.device)),
                        "cvqpg_loss_target_range")
+            self.target_moments = None
+            if cfg.target_moments:
+                self.target_moments = compute_target_moments(p, self.targets)
+                p.target_moments = _lib.ptr(self.target_moments)
         if init is None:
             init = synthetic_init(cfg, cfg.seed)
         self.load_raw(init)

@@ -26,7 +26,7 @@ class LossParams(ctypes.Structure):
     _fields_ = [("channels", ctypes.c_int), ("planes", ctypes.c_int), ("height", ctypes.c_int),
                 ("width", ctypes.c_int), ("w_l2", ctypes.c_float), ("w_mask", ctypes.c_float),
                 ("w_cor", ctypes.c_float), ("ssim_weight", ctypes.c_float), ("noise_ratio", ctypes.c_float),
-                ("inject_noise", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
+                ("inject_noise", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("target_moments", ctypes.c_void_p)]
 
 
 class MultiplaneLoss:
@@ -37,7 +37,7 @@ class MultiplaneLoss:
     """
 
     def __init__(self, targets, depth_plane, weights=(1.0, 1.0, 1.0), ssim_weight=0.025 * 0.2,
-                 noise_ratio=1e-3, inject_noise=True, seed=0):
+                 noise_ratio=1e-3, inject_noise=True, seed=0, target_moments=True):
         if targets.dim() != 4:
             raise ValueError("targets must be [planes, channels, height, width]")
         P, C, H, W = targets.shape
@@ -55,6 +55,14 @@ class MultiplaneLoss:
         _lib.check(lib.cvqpg_loss_target_range(_lib.ptr(self.targets), P, C, H, W, _lib.ptr(self.target_range),
                                                _lib.ptr(self.ws), self.ws.numel(), _lib.stream_of(self.device)),
                    "cvqpg_loss_target_range")
+        self.moments = None
+        if target_moments:  # the targets are fixed: filter them once (cvqpg_loss_target_moments)
+            nbytes = _lib.size_query(lib.cvqpg_loss_target_moments_size, ctypes.byref(self.prm))
+            self.moments = torch.empty(nbytes // 4, dtype=torch.float32, device=self.device)
+            _lib.check(lib.cvqpg_loss_target_moments(ctypes.byref(self.prm), _lib.ptr(self.targets),
+                                                     _lib.ptr(self.moments), nbytes, _lib.stream_of(self.device)),
+                       "cvqpg_loss_target_moments")
+            self.prm.target_moments = _lib.ptr(self.moments)
         self.shape = (P, C, H, W)
 
     def __call__(self, pred, iteration=0, out=None, grad_pred=None):

@@ -250,6 +250,10 @@ typedef struct cvqpg_loss_params {
     float noise_ratio;          /* reference 1e-3 (utils/propagator.py:417) */
     int inject_noise;           /* 1 in the fit loop (train_2d_gaussian_rgb.py:195) */
     unsigned long long seed;
+    /* Optional: SSIM moments of these targets from cvqpg_loss_target_moments, or NULL
+     * to filter the targets on every call. The targets are constant during a fit,
+     * so precomputing them leaves three of the five windowed moments per call. */
+    const float* target_moments;
 } cvqpg_loss_params;
 
 CVQPG_API int cvqpg_loss_workspace_size(const cvqpg_loss_params* prm, size_t* bytes);
@@ -259,6 +263,12 @@ CVQPG_API int cvqpg_loss_workspace_size(const cvqpg_loss_params* prm, size_t* by
 #define CVQPG_TARGET_RANGE_WORKSPACE_PER_PLANE 512
 CVQPG_API int cvqpg_loss_target_range(const float* targets, int planes, int channels, int height, int width,
                                       float* target_range, void* workspace, size_t workspace_bytes, void* stream);
+/* Windowed SSIM moments of the targets (same 11-tap window as the loss):
+ * float2 (mu_T, E_w[T^2]) per valid map position, [P*C][H-10][W-10]. Summed in the
+ * loss kernel's order, so the loss gives the same result with or without them. */
+CVQPG_API int cvqpg_loss_target_moments_size(const cvqpg_loss_params* prm, size_t* bytes);
+CVQPG_API int cvqpg_loss_target_moments(const cvqpg_loss_params* prm, const float* targets, float* moments,
+                                        size_t moments_bytes, void* stream);
 CVQPG_API int cvqpg_loss_forward_backward(const cvqpg_loss_params* prm, const float* pred, const float* targets,
                                           const uint8_t* depth_plane, const float* target_range,
                                           const int32_t* iteration, float* grad_pred, float* out,
@@ -319,6 +329,7 @@ typedef struct cvqpg_fit_params {
     float noise_ratio;      /* 1e-3 */
     int plan_hint;          /* FFT plan choice of the propagation, 0 = default (CVQPG_PLAN_*) */
     unsigned long long seed;
+    const float* target_moments; /* optional, as in cvqpg_loss_params (same targets) */
 } cvqpg_fit_params;
 
 CVQPG_API int cvqpg_fit_workspace_size(const cvqpg_fit_params* prm, size_t* bytes);

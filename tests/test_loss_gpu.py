@@ -75,3 +75,44 @@ def test_loss_rejects_bad_parameters():
                                          ctypes.byref(sz)) == 5  # more planes than supported
     assert lib.cvqpg_loss_workspace_size(ctypes.byref(LossParams(2, 3, 64, 64, 1, 1, 1, 0.005, 1e-3, 1, 0)),
                                          ctypes.byref(sz)) == 2  # channels
+
+
+@pytest.mark.parametrize("P,C,H,W", [(3, 3, 45, 70), (1, 1, 256, 256), (2, 3, 11, 11), (3, 1, 97, 161)])
+def test_target_moments_path_matches_on_the_fly(P, C, H, W):
+    """Precomputed target moments (cvqpg_loss_target_moments) against filtering the targets in the
+    loss call: same window, same fma order, so the results agree to float32 rounding (1e-6)."""
+    from complex_valued_quadratic_phase_gaussian_b200.loss import MultiplaneLoss
+    pred, targets, depth = _case(P, C, H, W, seed=77 + H)
+    t, d = torch.from_numpy(targets).cuda(), torch.from_numpy(depth).cuda()
+    a = MultiplaneLoss(t, d, seed=3, target_moments=True)
+    b = MultiplaneLoss(t, d, seed=3, target_moments=False)
+    assert a.moments is not None and b.moments is None
+    x = torch.from_numpy(pred).cuda()
+    oa, ga = a(x, iteration=11)
+    ob, gb = b(x, iteration=11)
+    torch.cuda.synchronize()
+    assert torch.allclose(oa, ob, rtol=1e-6, atol=0)
+    assert rel_l2(ga.cpu().numpy(), gb.cpu().numpy()) < 1e-6
+
+
+def test_target_moments_against_float64_window():
+    """cvqpg_loss_target_moments: (mu_T, E_w[T^2]) on the valid map, against a float64 11x11 window."""
+    from complex_valued_quadratic_phase_gaussian_b200.loss import MultiplaneLoss
+    P, C, H, W = 2, 3, 50, 77
+    _, targets, depth = _case(P, C, H, W, seed=12)
+    lf = MultiplaneLoss(torch.from_numpy(targets).cuda(), torch.from_numpy(depth).cuda())
+    torch.cuda.synchronize()
+    mom = lf.moments.view(P * C, H - 10, W - 10, 2).cpu().numpy().astype(np.float64)
+    g = np.exp(-((np.arange(11) - 5.0) ** 2) / (2 * 1.5 ** 2))
+    g /= g.sum()
+    w2 = np.outer(g, g)
+    T = targets.reshape(P * C, H, W).astype(np.float64)
+    mu = np.zeros((P * C, H - 10, W - 10))
+    e2 = np.zeros_like(mu)
+    for a in range(11):
+        for b in range(11):
+            win = T[:, a:a + H - 10, b:b + W - 10]
+            mu += w2[a, b] * win
+            e2 += w2[a, b] * win * win
+    np.testing.assert_allclose(mom[..., 0], mu, atol=2e-6)
+    np.testing.assert_allclose(mom[..., 1], e2, atol=2e-6)
