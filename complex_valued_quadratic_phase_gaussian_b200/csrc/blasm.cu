@@ -458,6 +458,7 @@ static bool column_split(const FftPlan& plan, ColSplit* cs, int radix_hint) {
 static void launch_columns(bool adjoint, const BlasmDev& d, const float2* in, float2* out, cudaStream_t s) {
     ColSplit cs;
     if (column_split(d.col, &cs, d.col_radix)) {
+        if (launch_cols_ct(adjoint, d, cs, in, out, s)) return;
         switch (cs.rl) {
             case 3: launch_cols_reg_r3(adjoint, d, cs, in, out, s); return;
             case 5: launch_cols_reg_r5(adjoint, d, cs, in, out, s); return;

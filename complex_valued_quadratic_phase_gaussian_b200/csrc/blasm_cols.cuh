@@ -93,6 +93,129 @@ struct ColSplit {
     int ntw;  // twiddle-table prefix the passes read (n / smallest radix), copied to shared memory
 };
 
+// ---------------------------------------------------------------------------
+// Head passes of the column FFT: every pass of the plan except the radix held
+// in registers. HeadRuntime follows the plan read at run time (any supported
+// length); HeadCT2<N, RA, RB> is a two-pass head fixed at compile time
+// (N = RA * RB * RL), so its strides, index splits and padded shared-memory
+// addresses fold into constants and no per-pass radix dispatch is compiled in.
+// ---------------------------------------------------------------------------
+// v[r] = x[j + r N/R] from a padded shared buffer
+template <int N, int R>
+struct SmemLoad {
+    const float2* in;
+    __device__ __forceinline__ void operator()(int j, float2 (&v)[R]) const {
+        constexpr int nb = N / R;
+        if constexpr (nb % 16 == 0) {  // (j + r nb) >> 4 = (j >> 4) + r nb / 16
+            const float2* p = in + fft_padT<kColPad>(j);
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = p[r * (nb + nb / 16)];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = in[fft_padT<kColPad>(j + r * nb)];
+        }
+    }
+};
+
+// y[o + r NS] = v[r] into a padded shared buffer
+template <int R, int NS>
+struct SmemStore {
+    float2* out;
+    __device__ __forceinline__ void operator()(int o, const float2 (&v)[R]) const {
+        if constexpr (NS % 16 == 0) {
+            float2* p = out + fft_padT<kColPad>(o);
+#pragma unroll
+            for (int r = 0; r < R; r++) p[r * (NS + NS / 16)] = v[r];
+        } else if constexpr (NS == 1 && 16 % R == 0) {  // o is a multiple of R: o..o+R-1 share a 16-block
+            float2* p = out + fft_padT<kColPad>(o);
+#pragma unroll
+            for (int r = 0; r < R; r++) p[r] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) out[fft_padT<kColPad>(o + r * NS)] = v[r];
+        }
+    }
+};
+
+// One Stockham pass with compile-time length, radix and stride (same formulation
+// as fft_pass): butterfly j, k = j mod NS, twiddle W_N^(r k N/(NS R)).
+template <int N, int R, int NS, bool INV, typename Load, typename Store>
+__device__ __forceinline__ void ct_pass(Load load, Store store, const float2* tw) {
+    constexpr int nb = N / R;
+    constexpr int stride = N / (NS * R);
+    for (int j = threadIdx.x; j < nb; j += kColThreads) {
+        const int q = j / NS, k = j - q * NS;
+        float2 v[R];
+        load(j, v);
+        if constexpr (NS > 1) {
+            float2 w = tw[k * stride];
+            if (INV) w.y = -w.y;
+            apply_twiddles<R>(v, w);
+        }
+        dft<R>(v, INV);
+        store(q * NS * R + k, v);
+    }
+    __syncthreads();
+}
+
+struct HeadRuntime {
+    static constexpr int kN = 0;
+    // forward head from stride 1 (first pass reads through src); returns the result buffer
+    template <typename Src>
+    __device__ static __forceinline__ float2* forward(Src src, float2* b0, float2* b1, int ld, int n,
+                                                      const ColSplit& cs, const float2* tw) {
+        return fft_run_passes<kColPad>(src, b0, b1, ld, 0, n, cs.head_code, cs.head_npass, 1, tw, false);
+    }
+    // inverse head from stride rl, input in b0, last pass through sink
+    template <typename Sink>
+    __device__ static __forceinline__ void inverse(Sink sink, float2* b0, float2* b1, int ld, int n, int rl,
+                                                   const ColSplit& cs, const float2* tw) {
+        fft_run_passes_to<kColPad>([b0](int, int e) { return b0[fft_padT<kColPad>(e)]; }, sink, b1, b0, ld, 0, n,
+                                   cs.head_code, cs.head_npass, rl, tw, true);
+    }
+};
+
+template <int N, int RA, int RB>
+struct HeadCT2 {
+    static constexpr int kN = N;
+    template <typename Src>
+    __device__ static __forceinline__ float2* forward(Src src, float2* b0, float2* b1, int, int, const ColSplit&,
+                                                      const float2* tw) {
+        ct_pass<N, RA, 1, false>(
+            [&](int j, float2 (&v)[RA]) {
+#pragma unroll
+                for (int r = 0; r < RA; r++) v[r] = src(0, j + r * (N / RA));
+            },
+            SmemStore<RA, 1>{b0}, tw);
+        ct_pass<N, RB, RA, false>(SmemLoad<N, RB>{b0}, SmemStore<RB, RA>{b1}, tw);
+        return b1;
+    }
+    template <typename Sink>
+    __device__ static __forceinline__ void inverse(Sink sink, float2* b0, float2* b1, int, int, int,
+                                                   const ColSplit&, const float2* tw) {
+        constexpr int RL = N / (RA * RB);
+        ct_pass<N, RA, RL, true>(SmemLoad<N, RA>{b0}, SmemStore<RA, RL>{b1}, tw);
+        ct_pass<N, RB, RL * RA, true>(
+            SmemLoad<N, RB>{b1},
+            [&](int o, const float2 (&v)[RB]) {
+#pragma unroll
+                for (int r = 0; r < RB; r++) sink(0, o + r * (RL * RA), v[r]);
+            },
+            tw);
+    }
+};
+
+// v[r] = buf[j + r nbL], the input of the register-held pass
+template <class Head, int RL>
+__device__ __forceinline__ void load_rl(const float2* buf, int j, int nbL, float2 (&v)[RL]) {
+    if constexpr (Head::kN > 0) {
+        SmemLoad<Head::kN, RL>{buf}(j, v);
+    } else {
+#pragma unroll
+        for (int r = 0; r < RL; r++) v[r] = buf[fft_padT<kColPad>(j + r * nbL)];
+    }
+}
+
 // K2 (register-spectrum variant): one column per CTA. Forward column FFT;
 // the last forward pass leaves its butterflies in registers together with the
 // plane-independent transfer excess E of each element; for each plane the first
@@ -100,12 +223,12 @@ struct ColSplit {
 // function straight from registers, and the last inverse pass writes the kept
 // rows to global memory. Shared memory: two FFT buffers, the twiddle prefix and
 // the excess of every element (-1 where no plane propagates it).
-template <int RL, int MB>
+template <int RL, int MB, class Head = HeadRuntime>
 __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(BlasmDev d, ColSplit cs,
                                                                          const float2* __restrict__ A,
                                                                          float2* __restrict__ B) {
     extern __shared__ float2 sm[];
-    const int NH = d.NH, NW = d.NW, ld = fft_ldT<kColPad>(NH);
+    const int NH = Head::kN > 0 ? Head::kN : d.NH, NW = d.NW, ld = fft_ldT<kColPad>(NH);
     float2* b0 = sm;
     float2* b1 = sm + ld;
     float2* tw = sm + 2 * ld;
@@ -115,12 +238,12 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
     const int c = blockIdx.x / NW, kx = blockIdx.x - c * NW;
     const int y0 = (NH >> 1) - (d.pH >> 1), pH = d.pH;
     const float2* src = A + (size_t)c * pH * NW + kx;
-    float2* buf = fft_run_passes<kColPad>(
+    float2* buf = Head::forward(
         [=](int, int e) {
             const int y = e - y0;
             return (y < 0 || y >= pH) ? make_float2(0.f, 0.f) : __ldg(&src[(size_t)y * NW]);
         },
-        b0, b1, ld, 0, NH, cs.head_code, cs.head_npass, 1, tw, false);
+        b0, b1, ld, NH, cs, tw);
     const int nbL = NH / RL;  // = stride Ns of the last pass; k = j, twiddle stride 1
     int ci = kx + (NW >> 1);
     if (ci >= NW) ci -= NW;
@@ -131,8 +254,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
         const int j = threadIdx.x + b * blockDim.x;
         if (j < nbL) {
             float2 v[RL];
-#pragma unroll
-            for (int r = 0; r < RL; r++) v[r] = buf[fft_padT<kColPad>(j + r * nbL)];
+            load_rl<Head, RL>(buf, j, nbL, v);
             apply_twiddles<RL>(v, tw[j]);
             dft<RL>(v, false);
 #pragma unroll
@@ -165,18 +287,17 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
                     v[r] = on ? cmul(spec[b][r], transfer_from_excess(pp, E, d.scale)) : make_float2(0.f, 0.f);
                 }
                 dft<RL>(v, true);
-#pragma unroll
-                for (int r = 0; r < RL; r++) b0[fft_padT<kColPad>(j * RL + r)] = v[r];
+                SmemStore<RL, 1>{b0}(j * RL, v);
             }
         }
         __syncthreads();
         float2* dst = B + (size_t)pc * oh * NW + kx;
-        fft_run_passes_to<kColPad>([b0](int, int e) { return b0[fft_padT<kColPad>(e)]; },
-                          [=](int, int a, float2 v) {
-                              const int y = a - row0;
-                              if ((unsigned)y < (unsigned)oh) dst[(size_t)y * NW] = v;
-                          },
-                          b1, b0, ld, 0, NH, cs.head_code, cs.head_npass, RL, tw, true);
+        Head::inverse(
+            [=](int, int a, float2 v) {
+                const int y = a - row0;
+                if ((unsigned)y < (unsigned)oh) dst[(size_t)y * NW] = v;
+            },
+            b0, b1, ld, NH, RL, cs, tw);
     }
 }
 
@@ -184,12 +305,12 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
 // its butterflies in registers, multiplied by conj(transfer) and accumulated
 // there; then the first inverse pass starts from the accumulator and the last
 // one writes the kept rows to global memory.
-template <int RL, int MB>
+template <int RL, int MB, class Head = HeadRuntime>
 __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(BlasmDev d, ColSplit cs,
                                                                          const float2* __restrict__ Bt,
                                                                          float2* __restrict__ Ab) {
     extern __shared__ float2 sm[];
-    const int NH = d.NH, NW = d.NW, ld = fft_ldT<kColPad>(NH);
+    const int NH = Head::kN > 0 ? Head::kN : d.NH, NW = d.NW, ld = fft_ldT<kColPad>(NH);
     float2* b0 = sm;
     float2* b1 = sm + ld;
     float2* tw = sm + 2 * ld;
@@ -216,12 +337,12 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
     for (int p = 0; p < d.P; p++) {
         const int pc = p * d.C + c;
         const float2* src = Bt + (size_t)pc * oh * NW + kx;
-        float2* buf = fft_run_passes<kColPad>(
+        float2* buf = Head::forward(
             [=](int, int e) {
                 const int y = e - row0;
                 return (y < 0 || y >= oh) ? make_float2(0.f, 0.f) : __ldg(&src[(size_t)y * NW]);
             },
-            b0, b1, ld, 0, NH, cs.head_code, cs.head_npass, 1, tw, false);
+            b0, b1, ld, NH, cs, tw);
         const PCParam pp = d.pcp[pc];
         const bool col_ok = ci >= pp.i0 && ci < pp.i1;
 #pragma unroll
@@ -229,8 +350,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
             const int j = threadIdx.x + b * blockDim.x;
             if (j < nbL) {
                 float2 v[RL];
-#pragma unroll
-                for (int r = 0; r < RL; r++) v[r] = buf[fft_padT<kColPad>(j + r * nbL)];
+                load_rl<Head, RL>(buf, j, nbL, v);
                 apply_twiddles<RL>(v, tw[j]);
                 dft<RL>(v, false);
                 if (col_ok) {
@@ -255,20 +375,19 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
 #pragma unroll
             for (int r = 0; r < RL; r++) v[r] = acc[b][r];
             dft<RL>(v, true);
-#pragma unroll
-            for (int r = 0; r < RL; r++) b0[fft_padT<kColPad>(j * RL + r)] = v[r];
+            SmemStore<RL, 1>{b0}(j * RL, v);
         }
     }
     __syncthreads();
     const int in_h = d.input_mode == 0 ? d.H : d.pH;
     const int r0 = (NH >> 1) - (in_h >> 1);
     float2* dst = Ab + (size_t)c * in_h * NW + kx;
-    fft_run_passes_to<kColPad>([b0](int, int e) { return b0[fft_padT<kColPad>(e)]; },
-                      [=](int, int a, float2 v) {
-                          const int y = a - r0;
-                          if ((unsigned)y < (unsigned)in_h) dst[(size_t)y * NW] = v;
-                      },
-                      b1, b0, ld, 0, NH, cs.head_code, cs.head_npass, RL, tw, true);
+    Head::inverse(
+        [=](int, int a, float2 v) {
+            const int y = a - r0;
+            if ((unsigned)y < (unsigned)in_h) dst[(size_t)y * NW] = v;
+        },
+        b0, b1, ld, NH, RL, cs, tw);
 }
 
 
@@ -287,32 +406,34 @@ void launch_cols_reg_r13(bool adjoint, const BlasmDev& d, const ColSplit& cs, co
 void launch_cols_reg_r16(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
                          cudaStream_t s);
 
+template <int RL, int MB, class Head>
+void launch_cols_reg_t(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                       cudaStream_t s) {
+    const size_t sm = ((size_t)2 * fft_ldT<kColPad>(d.NH) + cs.ntw) * sizeof(float2) + (size_t)d.NH * sizeof(float);
+    if (!adjoint) {
+        cudaFuncSetAttribute(blasm_cols_fwd_reg_kernel<RL, MB, Head>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm);
+        blasm_cols_fwd_reg_kernel<RL, MB, Head><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);
+    } else {
+        cudaFuncSetAttribute(blasm_cols_adj_reg_kernel<RL, MB, Head>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm);
+        blasm_cols_adj_reg_kernel<RL, MB, Head><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);
+    }
+}
+
+// Column kernels with a compile-time head for the grids the fit uses most; false
+// when (d, cs) is not one of them (the run-time plan variants apply).
+bool launch_cols_ct(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                    cudaStream_t s);
+
 // Instantiate the forward and adjoint register-spectrum kernels for one radix.
 #define CVQPG_DEFINE_COLS_REG(RL)                                                                                  \
     void launch_cols_reg_r##RL(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out, \
                                cudaStream_t s) {                                                                   \
-        const size_t sm = ((size_t)2 * fft_ldT<kColPad>(d.NH) + cs.ntw) * sizeof(float2) + (size_t)d.NH * sizeof(float);                                              \
-        if (!adjoint) {                                                                                            \
-            if (cs.mb == 1) {                                                                                      \
-                cudaFuncSetAttribute(blasm_cols_fwd_reg_kernel<RL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                     (int)sm);                                                                     \
-                blasm_cols_fwd_reg_kernel<RL, 1><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);              \
-            } else {                                                                                               \
-                cudaFuncSetAttribute(blasm_cols_fwd_reg_kernel<RL, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                     (int)sm);                                                                     \
-                blasm_cols_fwd_reg_kernel<RL, 2><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);              \
-            }                                                                                                      \
-        } else {                                                                                                   \
-            if (cs.mb == 1) {                                                                                      \
-                cudaFuncSetAttribute(blasm_cols_adj_reg_kernel<RL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                     (int)sm);                                                                     \
-                blasm_cols_adj_reg_kernel<RL, 1><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);              \
-            } else {                                                                                               \
-                cudaFuncSetAttribute(blasm_cols_adj_reg_kernel<RL, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                     (int)sm);                                                                     \
-                blasm_cols_adj_reg_kernel<RL, 2><<<d.C * d.NW, kColThreads, sm, s>>>(d, cs, in, out);              \
-            }                                                                                                      \
-        }                                                                                                          \
+        if (cs.mb == 1)                                                                                            \
+            launch_cols_reg_t<RL, 1, HeadRuntime>(adjoint, d, cs, in, out, s);                                     \
+        else                                                                                                       \
+            launch_cols_reg_t<RL, 2, HeadRuntime>(adjoint, d, cs, in, out, s);                                     \
     }
 
 }  // namespace cvqpg
