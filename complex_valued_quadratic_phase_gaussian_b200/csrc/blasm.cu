@@ -77,8 +77,36 @@ bool make_fft_plan(int n, FftPlan* plan, int order) {
 // handled by neighbouring CTAs at the same time, so the 32-byte sectors are
 // completed in L2.
 // ---------------------------------------------------------------------------
+// Row FFT policies: RowRuntime runs the plan read at run time; RowCT<N, R...>
+// the plan fixed at compile time (CtFft), for the row length of the 1080p fit.
+struct RowRuntime {
+    template <bool INV, typename Src>
+    __device__ static __forceinline__ float2* run(Src src, float2* b0, float2* b1, int ld, const BlasmDev& d) {
+        return fft_run(src, b0, b1, ld, 0, d.row, INV);
+    }
+};
+
+template <int N, int... R>
+struct RowCT {
+    static constexpr int kPasses = (int)sizeof...(R);
+    template <bool INV, typename Src>
+    __device__ static __forceinline__ float2* run(Src src, float2* b0, float2* b1, int, const BlasmDev& d) {
+        float2* res = (kPasses % 2 == 1) ? b0 : b1;  // the buffer the last pass does not read
+        CtFft<5, kRowThreads, N, INV, 1, R...>::run(ElemLoadF<Src>{src}, SmemStoreF<5>{res}, b0, b1, d.row.tw);
+        return res;
+    }
+};
+
+// The 1080p fit's rows: 2 x 2240 = 4480 = 16 x 8 x 5 x 7 (the default radix order).
+using Row4480 = RowCT<4480, 16, 8, 5, 7>;
+static bool row_is_4480(const BlasmDev& d) {
+    const unsigned long long code = 16ull | (8ull << 5) | (5ull << 10) | (7ull << 15);
+    return d.NW == 4480 && d.row.npass == 4 && d.row.code == code;
+}
+
 // K1: one padded row per CTA. The first FFT pass reads the splat field directly
 // (replicate guard band, Tukey window, amplitude clamp on the fly).
+template <class RF = RowRuntime>
 __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_kernel(BlasmDev d, const float2* __restrict__ in,
                                                                      float2* __restrict__ A) {
     extern __shared__ float2 sm[];
@@ -95,7 +123,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_kernel(BlasmDev
         const float2* src = in + ((size_t)c * d.H + yy) * d.W;
         const float* wx = d.wx;
         const int pad_w = d.pad_w, W = d.W;
-        res = fft_run(
+        res = RF::template run<false>(
             [=](int, int e) {
                 const int x = e - x0;
                 if (x < 0 || x >= pW) return make_float2(0.f, 0.f);
@@ -104,15 +132,15 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_kernel(BlasmDev
                 const float2 u = __ldg(&src[xx]);
                 return clamp_amplitude(make_float2(u.x * w, u.y * w));
             },
-            b0, b1, ld, 0, d.row, false);
+            b0, b1, ld, d);
     } else {
         const float2* src = in + ((size_t)c * d.pH + y) * d.pW;
-        res = fft_run(
+        res = RF::template run<false>(
             [=](int, int e) {
                 const int x = e - x0;
                 return (x < 0 || x >= pW) ? make_float2(0.f, 0.f) : __ldg(&src[x]);
             },
-            b0, b1, ld, 0, d.row, false);
+            b0, b1, ld, d);
     }
     float2* dst = A + ((size_t)c * d.pH + y) * d.NW;
     for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) dst[kx] = res[fft_pad(kx)];
@@ -150,6 +178,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_kernel(BlasmDev
 
 // K3: inverse FFT of a kept row (first pass reads global), keep out_w columns
 // -> V [P*C][out_h][out_w] and optionally pred = clamp(|V|^2, 0, 1)
+template <class RF = RowRuntime>
 __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_kernel(BlasmDev d, const float2* __restrict__ B,
                                                                      float2* __restrict__ V,
                                                                      float* __restrict__ pred) {
@@ -157,7 +186,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_kernel(BlasmDev
     const int ld = fft_ld(d.NW);
     const size_t row = blockIdx.x;  // pc * out_h + y
     const float2* src = B + row * d.NW;
-    float2* res = fft_run([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, 0, d.row, true);
+    float2* res = RF::template run<true>([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, d);
     const int col0 = (d.NW >> 1) - (d.out_w >> 1);
     float2* dst = V + row * d.out_w;
     if (pred) {
@@ -177,6 +206,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_kernel(BlasmDev
 // adjoint kernels (same layouts: Bt [P*C][out_h][NW], Ab [C][in_h][NW])
 // ---------------------------------------------------------------------------
 // K3b: gradient row embedded at the out_w centred columns -> forward FFT
+template <class RF = RowRuntime>
 __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_adj_kernel(BlasmDev d, const float2* __restrict__ gV,
                                                                          const float* __restrict__ gpred,
                                                                          const float2* __restrict__ Vf,
@@ -191,7 +221,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_adj_kernel(Blas
         // dL/dV = 2 V dL/dpred where 0 <= |V|^2 <= 1 (clamp passes its bounds), else 0
         const float* gp = gpred + (size_t)row * ow;
         const float2* vv = Vf + (size_t)row * ow;
-        res = fft_run(
+        res = RF::template run<false>(
             [=](int, int e) {
                 const int x = e - col0;
                 if (x < 0 || x >= ow) return make_float2(0.f, 0.f);
@@ -201,15 +231,15 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_adj_kernel(Blas
                 const float g = (v.x * v.x + v.y * v.y <= 1.0f) ? 2.0f * gpx : 0.0f;
                 return make_float2(g * v.x, g * v.y);
             },
-            sm, sm + ld, ld, 0, d.row, false);
+            sm, sm + ld, ld, d);
     } else {
         const float2* src = gV + (size_t)row * ow;
-        res = fft_run(
+        res = RF::template run<false>(
             [=](int, int e) {
                 const int x = e - col0;
                 return (x < 0 || x >= ow) ? make_float2(0.f, 0.f) : __ldg(&src[x]);
             },
-            sm, sm + ld, ld, 0, d.row, false);
+            sm, sm + ld, ld, d);
     }
     float2* dst = Bt + (size_t)row * d.NW;
     for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) dst[kx] = res[fft_pad(kx)];
@@ -260,6 +290,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_kernel(BlasmDev
 
 // K1b: inverse row FFT (first pass reads global), keep the input columns,
 // apply the amplitude-clamp adjoint against the splat field
+template <class RF = RowRuntime>
 __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_adj_kernel(BlasmDev d, const float2* __restrict__ Ab,
                                                                          const float2* __restrict__ field,
                                                                          float2* __restrict__ gin) {
@@ -267,7 +298,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_adj_kernel(Blas
     const int ld = fft_ld(d.NW);
     const int row = blockIdx.x;  // c * in_h + y
     const float2* src = Ab + (size_t)row * d.NW;
-    float2* res = fft_run([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, 0, d.row, true);
+    float2* res = RF::template run<true>([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, d);
     const int in_w = d.input_mode == 0 ? d.W : d.pW;
     const int c0 = (d.NW >> 1) - (in_w >> 1);
     float2* dst = gin + (size_t)row * in_w;
@@ -490,18 +521,47 @@ static void launch_columns(bool adjoint, const BlasmDev& d, const float2* in, fl
     }
 }
 
+template <class RF>
+static void rows_forward(const BlasmDev& d, const float2* in, float2* A, cudaStream_t s) {
+    const size_t rs = row_smem(d);
+    CVQPG_SMEM_ATTR(blasm_rows_fwd_kernel<RF>, rs);
+    blasm_rows_fwd_kernel<RF><<<d.C * d.pH, kRowThreads, rs, s>>>(d, in, A);
+}
+
+template <class RF>
+static void rows_inverse(const BlasmDev& d, const float2* B, float2* out, float* pred, cudaStream_t s) {
+    const size_t rs = row_smem(d);
+    CVQPG_SMEM_ATTR(blasm_rows_inv_kernel<RF>, rs);
+    blasm_rows_inv_kernel<RF><<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, B, out, pred);
+}
+
+template <class RF>
+static void rows_forward_adjoint(const BlasmDev& d, const float2* grad_out, const float* grad_pred,
+                                 const float2* vfield, float2* B, cudaStream_t s) {
+    const size_t rs = row_smem(d);
+    CVQPG_SMEM_ATTR(blasm_rows_fwd_adj_kernel<RF>, rs);
+    blasm_rows_fwd_adj_kernel<RF><<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, grad_out, grad_pred, vfield, B);
+}
+
+template <class RF>
+static void rows_inverse_adjoint(const BlasmDev& d, const float2* A, const float2* in_field, float2* grad_in,
+                                 cudaStream_t s) {
+    const size_t rs = row_smem(d);
+    const int in_h = d.input_mode == 0 ? d.H : d.pH;
+    CVQPG_SMEM_ATTR(blasm_rows_inv_adj_kernel<RF>, rs);
+    blasm_rows_inv_adj_kernel<RF><<<d.C * in_h, kRowThreads, rs, s>>>(d, A, in_field, grad_in);
+}
+
 void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace, cudaStream_t s,
                    StageMarks* marks) {
     float2 *A, *B;
     carve(d, workspace, &A, &B);
-    const size_t rs = row_smem(d);
-    CVQPG_SMEM_ATTR(blasm_rows_fwd_kernel, rs);
-    blasm_rows_fwd_kernel<<<d.C * d.pH, kRowThreads, rs, s>>>(d, in, A);
+    const bool ct = row_is_4480(d);
+    if (ct) rows_forward<Row4480>(d, in, A, s); else rows_forward<RowRuntime>(d, in, A, s);
     if (marks) marks->mark(s);
     launch_columns(false, d, A, B, s);
     if (marks) marks->mark(s);
-    CVQPG_SMEM_ATTR(blasm_rows_inv_kernel, rs);
-    blasm_rows_inv_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, B, out, pred);
+    if (ct) rows_inverse<Row4480>(d, B, out, pred, s); else rows_inverse<RowRuntime>(d, B, out, pred, s);
     if (marks) marks->mark(s);
 }
 
@@ -509,15 +569,16 @@ void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* gra
                     const float2* vfield, float2* grad_in, void* workspace, cudaStream_t s, StageMarks* marks) {
     float2 *A, *B;
     carve(d, workspace, &A, &B);
-    const size_t rs = row_smem(d);
-    CVQPG_SMEM_ATTR(blasm_rows_fwd_adj_kernel, rs);
-    blasm_rows_fwd_adj_kernel<<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, grad_out, grad_pred, vfield, B);
+    const bool ct = row_is_4480(d);
+    if (ct)
+        rows_forward_adjoint<Row4480>(d, grad_out, grad_pred, vfield, B, s);
+    else
+        rows_forward_adjoint<RowRuntime>(d, grad_out, grad_pred, vfield, B, s);
     if (marks) marks->mark(s);
     launch_columns(true, d, B, A, s);
     if (marks) marks->mark(s);
-    const int in_h = d.input_mode == 0 ? d.H : d.pH;
-    CVQPG_SMEM_ATTR(blasm_rows_inv_adj_kernel, rs);
-    blasm_rows_inv_adj_kernel<<<d.C * in_h, kRowThreads, rs, s>>>(d, A, in_field, grad_in);
+    if (ct) rows_inverse_adjoint<Row4480>(d, A, in_field, grad_in, s);
+    else rows_inverse_adjoint<RowRuntime>(d, A, in_field, grad_in, s);
     if (marks) marks->mark(s);
 }
 

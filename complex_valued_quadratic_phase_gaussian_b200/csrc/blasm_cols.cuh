@@ -100,64 +100,6 @@ struct ColSplit {
 // (N = RA * RB * RL), so its strides, index splits and padded shared-memory
 // addresses fold into constants and no per-pass radix dispatch is compiled in.
 // ---------------------------------------------------------------------------
-// v[r] = x[j + r N/R] from a padded shared buffer
-template <int N, int R>
-struct SmemLoad {
-    const float2* in;
-    __device__ __forceinline__ void operator()(int j, float2 (&v)[R]) const {
-        constexpr int nb = N / R;
-        if constexpr (nb % 16 == 0) {  // (j + r nb) >> 4 = (j >> 4) + r nb / 16
-            const float2* p = in + fft_padT<kColPad>(j);
-#pragma unroll
-            for (int r = 0; r < R; r++) v[r] = p[r * (nb + nb / 16)];
-        } else {
-#pragma unroll
-            for (int r = 0; r < R; r++) v[r] = in[fft_padT<kColPad>(j + r * nb)];
-        }
-    }
-};
-
-// y[o + r NS] = v[r] into a padded shared buffer
-template <int R, int NS>
-struct SmemStore {
-    float2* out;
-    __device__ __forceinline__ void operator()(int o, const float2 (&v)[R]) const {
-        if constexpr (NS % 16 == 0) {
-            float2* p = out + fft_padT<kColPad>(o);
-#pragma unroll
-            for (int r = 0; r < R; r++) p[r * (NS + NS / 16)] = v[r];
-        } else if constexpr (NS == 1 && 16 % R == 0) {  // o is a multiple of R: o..o+R-1 share a 16-block
-            float2* p = out + fft_padT<kColPad>(o);
-#pragma unroll
-            for (int r = 0; r < R; r++) p[r] = v[r];
-        } else {
-#pragma unroll
-            for (int r = 0; r < R; r++) out[fft_padT<kColPad>(o + r * NS)] = v[r];
-        }
-    }
-};
-
-// One Stockham pass with compile-time length, radix and stride (same formulation
-// as fft_pass): butterfly j, k = j mod NS, twiddle W_N^(r k N/(NS R)).
-template <int N, int R, int NS, bool INV, typename Load, typename Store>
-__device__ __forceinline__ void ct_pass(Load load, Store store, const float2* tw) {
-    constexpr int nb = N / R;
-    constexpr int stride = N / (NS * R);
-    for (int j = threadIdx.x; j < nb; j += kColThreads) {
-        const int q = j / NS, k = j - q * NS;
-        float2 v[R];
-        load(j, v);
-        if constexpr (NS > 1) {
-            float2 w = tw[k * stride];
-            if (INV) w.y = -w.y;
-            apply_twiddles<R>(v, w);
-        }
-        dft<R>(v, INV);
-        store(q * NS * R + k, v);
-    }
-    __syncthreads();
-}
-
 struct HeadRuntime {
     static constexpr int kN = 0;
     // forward head from stride 1 (first pass reads through src); returns the result buffer
@@ -181,27 +123,16 @@ struct HeadCT2 {
     template <typename Src>
     __device__ static __forceinline__ float2* forward(Src src, float2* b0, float2* b1, int, int, const ColSplit&,
                                                       const float2* tw) {
-        ct_pass<N, RA, 1, false>(
-            [&](int j, float2 (&v)[RA]) {
-#pragma unroll
-                for (int r = 0; r < RA; r++) v[r] = src(0, j + r * (N / RA));
-            },
-            SmemStore<RA, 1>{b0}, tw);
-        ct_pass<N, RB, RA, false>(SmemLoad<N, RB>{b0}, SmemStore<RB, RA>{b1}, tw);
+        CtFft<kColPad, kColThreads, N, false, 1, RA, RB>::run(ElemLoadF<Src>{src}, SmemStoreF<kColPad>{b1}, b0, b1,
+                                                              tw);
         return b1;
     }
     template <typename Sink>
     __device__ static __forceinline__ void inverse(Sink sink, float2* b0, float2* b1, int, int, int,
                                                    const ColSplit&, const float2* tw) {
         constexpr int RL = N / (RA * RB);
-        ct_pass<N, RA, RL, true>(SmemLoad<N, RA>{b0}, SmemStore<RA, RL>{b1}, tw);
-        ct_pass<N, RB, RL * RA, true>(
-            SmemLoad<N, RB>{b1},
-            [&](int o, const float2 (&v)[RB]) {
-#pragma unroll
-                for (int r = 0; r < RB; r++) sink(0, o + r * (RL * RA), v[r]);
-            },
-            tw);
+        CtFft<kColPad, kColThreads, N, true, RL, RA, RB>::run(SmemLoadF<kColPad>{b0}, ElemStoreF<Sink>{sink}, b1,
+                                                               b0, tw);
     }
 };
 
@@ -209,7 +140,7 @@ struct HeadCT2 {
 template <class Head, int RL>
 __device__ __forceinline__ void load_rl(const float2* buf, int j, int nbL, float2 (&v)[RL]) {
     if constexpr (Head::kN > 0) {
-        SmemLoad<Head::kN, RL>{buf}(j, v);
+        SmemLoadF<kColPad>{buf}.template get<Head::kN, RL>(j, v);
     } else {
 #pragma unroll
         for (int r = 0; r < RL; r++) v[r] = buf[fft_padT<kColPad>(j + r * nbL)];
@@ -287,7 +218,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
                     v[r] = on ? cmul(spec[b][r], transfer_from_excess(pp, E, d.scale)) : make_float2(0.f, 0.f);
                 }
                 dft<RL>(v, true);
-                SmemStore<RL, 1>{b0}(j * RL, v);
+                SmemStoreF<kColPad>{b0}.template put<1, RL>(j * RL, v);
             }
         }
         __syncthreads();
@@ -375,7 +306,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
 #pragma unroll
             for (int r = 0; r < RL; r++) v[r] = acc[b][r];
             dft<RL>(v, true);
-            SmemStore<RL, 1>{b0}(j * RL, v);
+            SmemStoreF<kColPad>{b0}.template put<1, RL>(j * RL, v);
         }
     }
     __syncthreads();

@@ -277,6 +277,109 @@ __device__ __forceinline__ void fft_run_to(First first, Last last, float2* a, fl
     fft_run_passes_to(first, last, a, b, ld, tshift, plan.n, plan.code, plan.npass, 1, plan.tw, inv);
 }
 
+// ---------------------------------------------------------------------------
+// Compile-time plans: the same Stockham passes with the length, the radices and
+// the strides as template constants, so a kernel instantiated for one grid has
+// no per-pass radix dispatch and its index splits, strides and padded
+// addresses fold into constants. NT = threads of the CTA.
+//   load.get<N, R>(j, v):   v[r] = x[j + r N/R]
+//   store.put<NS, R>(o, v): y[o + r NS] = v[r]
+// ---------------------------------------------------------------------------
+template <int PS>
+struct SmemLoadF {  // padded shared buffer (fft_padT<PS>)
+    const float2* in;
+    template <int N, int R>
+    __device__ __forceinline__ void get(int j, float2 (&v)[R]) const {
+        constexpr int nb = N / R, blk = 1 << PS;
+        if constexpr (nb % blk == 0) {  // (j + r nb) >> PS = (j >> PS) + r nb / blk
+            const float2* p = in + fft_padT<PS>(j);
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = p[r * (nb + nb / blk)];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = in[fft_padT<PS>(j + r * nb)];
+        }
+    }
+};
+
+template <int PS>
+struct SmemStoreF {
+    float2* out;
+    template <int NS, int R>
+    __device__ __forceinline__ void put(int o, const float2 (&v)[R]) const {
+        constexpr int blk = 1 << PS;
+        if constexpr (NS % blk == 0) {
+            float2* p = out + fft_padT<PS>(o);
+#pragma unroll
+            for (int r = 0; r < R; r++) p[r * (NS + NS / blk)] = v[r];
+        } else if constexpr (NS == 1 && blk % R == 0) {  // o is a multiple of R: o..o+R-1 share a block
+            float2* p = out + fft_padT<PS>(o);
+#pragma unroll
+            for (int r = 0; r < R; r++) p[r] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) out[fft_padT<PS>(o + r * NS)] = v[r];
+        }
+    }
+};
+
+template <typename Src>
+struct ElemLoadF {  // element reads through src(0, e) (global loads with a fused pointwise op)
+    Src src;
+    template <int N, int R>
+    __device__ __forceinline__ void get(int j, float2 (&v)[R]) const {
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = src(0, j + r * (N / R));
+    }
+};
+
+template <typename Sink>
+struct ElemStoreF {  // element writes through sink(0, a, v)
+    Sink sink;
+    template <int NS, int R>
+    __device__ __forceinline__ void put(int o, const float2 (&v)[R]) const {
+#pragma unroll
+        for (int r = 0; r < R; r++) sink(0, o + r * NS, v[r]);
+    }
+};
+
+template <int NT, int N, int R, int NS, bool INV, typename Load, typename Store>
+__device__ __forceinline__ void ct_pass(const Load& load, const Store& store, const float2* tw) {
+    constexpr int nb = N / R;
+    constexpr int stride = N / (NS * R);
+    for (int j = threadIdx.x; j < nb; j += NT) {
+        const int q = j / NS, k = j - q * NS;
+        float2 v[R];
+        load.template get<N, R>(j, v);
+        if constexpr (NS > 1) {
+            float2 w = tw[k * stride];
+            if (INV) w.y = -w.y;
+            apply_twiddles<R>(v, w);
+        }
+        dft<R>(v, INV);
+        store.template put<NS, R>(q * NS * R + k, v);
+    }
+    __syncthreads();
+}
+
+// Passes R, Rest... of length N from stride NS: the first reads through `load`,
+// the intermediate ones ping-pong a -> b -> a ..., the last writes through `last`
+// (which must not be the buffer the last pass reads: buffer (passes - 2) % 2).
+template <int PS, int NT, int N, bool INV, int NS, int R, int... Rest>
+struct CtFft {
+    static constexpr int kPasses = 1 + (int)sizeof...(Rest);
+    template <typename Load, typename Store>
+    __device__ static __forceinline__ void run(const Load& load, const Store& last, float2* a, float2* b,
+                                               const float2* tw) {
+        if constexpr (sizeof...(Rest) == 0) {
+            ct_pass<NT, N, R, NS, INV>(load, last, tw);
+        } else {
+            ct_pass<NT, N, R, NS, INV>(load, SmemStoreF<PS>{a}, tw);
+            CtFft<PS, NT, N, INV, NS * R, Rest...>::run(SmemLoadF<PS>{a}, last, b, a, tw);
+        }
+    }
+};
+
 // Host: factor n into supported radices in one of four orders (0: 16/8/4/2
 // first, then 3..17; 1: odd radices first, largest first, then 16/8/4/2;
 // 2: 8/4/2 only, then odd; 3: odd first, then 8/4/2). Returns false when n has

@@ -110,10 +110,11 @@ def test_rgb_1080p_three_planes_vs_oracle():
     assert rel_l2(gf, go) < 2e-5
 
 
-def test_rgb_1080p_compile_time_column_plan_matches_run_time_plan():
-    """At the 2816-row column grid the default plan (16 x 16 x 11, radix 11 in registers) runs the
-    column kernels whose passes are fixed at compile time; keeping radix 16 in registers instead
-    (plan_hint 16) runs the run-time plan. Forward and adjoint agree within 1e-5 relative L2."""
+def test_rgb_1080p_compile_time_plans_match_run_time_plans():
+    """At the 1080p grid (2816 x 4480) the default plan runs the kernels whose FFT passes are fixed
+    at compile time (columns 16 x 16 x 11 with radix 11 in registers, rows 16 x 8 x 5 x 7).
+    plan_hint 16 (radix 16 in registers) runs the run-time column plan, plan_hint 2 << 8 (row
+    radices 8/4/2 first) the run-time row plan. Forward and adjoint agree within 1e-5 relative L2."""
     from complex_valued_quadratic_phase_gaussian_b200.propagator import (BlasmPlan, reference_distances,
                                                                          reference_pad_size)
     rng = np.random.default_rng(5)
@@ -126,7 +127,8 @@ def test_rgb_1080p_compile_time_column_plan_matches_run_time_plan():
     f = torch.from_numpy(_random_field(rng, 3, H, W)).cuda()
     g = torch.from_numpy((rng.normal(size=(3, 3, H, W)) + 1j * rng.normal(size=(3, 3, H, W))).astype(np.complex64))
     g = g.cuda()
-    va, vb = a.forward(f).cpu().numpy(), b.forward(f).cpu().numpy()
-    ga, gb = a.backward(f, g).cpu().numpy(), b.backward(f, g).cpu().numpy()
-    assert rel_l2(va, vb) < 1e-5
-    assert rel_l2(ga, gb) < 1e-5
+    c = BlasmPlan(3, H, W, pad, wl, dist, 3.74e-6, aperture_radius=19200, plan_hint=2 << 8)
+    va, vb, vc = (p.forward(f).cpu().numpy() for p in (a, b, c))
+    ga, gb, gc = (p.backward(f, g).cpu().numpy() for p in (a, b, c))
+    assert rel_l2(va, vb) < 1e-5 and rel_l2(va, vc) < 1e-5
+    assert rel_l2(ga, gb) < 1e-5 and rel_l2(ga, gc) < 1e-5
