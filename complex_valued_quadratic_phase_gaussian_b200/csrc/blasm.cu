@@ -80,25 +80,29 @@ bool make_fft_plan(int n, FftPlan* plan, int order) {
 // Row FFT policies: RowRuntime runs the plan read at run time; RowCT<N, R...>
 // the plan fixed at compile time (CtFft), for the row length of the 1080p fit.
 struct RowRuntime {
+    static constexpr int kThreads = kRowThreads;
     template <bool INV, typename Src>
     __device__ static __forceinline__ float2* run(Src src, float2* b0, float2* b1, int ld, const BlasmDev& d) {
         return fft_run(src, b0, b1, ld, 0, d.row, INV);
     }
 };
 
-template <int N, int... R>
+template <int NT, int N, int... R>
 struct RowCT {
+    static constexpr int kThreads = NT;
     static constexpr int kPasses = (int)sizeof...(R);
     template <bool INV, typename Src>
     __device__ static __forceinline__ float2* run(Src src, float2* b0, float2* b1, int, const BlasmDev& d) {
         float2* res = (kPasses % 2 == 1) ? b0 : b1;  // the buffer the last pass does not read
-        CtFft<5, kRowThreads, N, INV, 1, R...>::run(ElemLoadF<Src>{src}, SmemStoreF<5>{res}, b0, b1, d.row.tw);
+        CtFft<5, NT, N, INV, 1, R...>::run(ElemLoadF<Src>{src}, SmemStoreF<5>{res}, b0, b1, d.row.tw);
         return res;
     }
 };
 
-// The 1080p fit's rows: 2 x 2240 = 4480 = 16 x 8 x 5 x 7 (the default radix order).
-using Row4480 = RowCT<4480, 16, 8, 5, 7>;
+// The 1080p fit's rows: 2 x 2240 = 4480 = 16 x 8 x 5 x 7 (the default radix order);
+// 320 threads = 280, 560, 896, 640 butterflies in 1, 2, 3, 2 rounds.
+constexpr int kRow4480Threads = 320;
+using Row4480 = RowCT<kRow4480Threads, 4480, 16, 8, 5, 7>;
 static bool row_is_4480(const BlasmDev& d) {
     const unsigned long long code = 16ull | (8ull << 5) | (5ull << 10) | (7ull << 15);
     return d.NW == 4480 && d.row.npass == 4 && d.row.code == code;
@@ -107,7 +111,7 @@ static bool row_is_4480(const BlasmDev& d) {
 // K1: one padded row per CTA. The first FFT pass reads the splat field directly
 // (replicate guard band, Tukey window, amplitude clamp on the fly).
 template <class RF = RowRuntime>
-__global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_kernel(BlasmDev d, const float2* __restrict__ in,
+__global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_fwd_kernel(BlasmDev d, const float2* __restrict__ in,
                                                                      float2* __restrict__ A) {
     extern __shared__ float2 sm[];
     const int ld = fft_ld(d.NW);
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_kernel(BlasmDev
 // K3: inverse FFT of a kept row (first pass reads global), keep out_w columns
 // -> V [P*C][out_h][out_w] and optionally pred = clamp(|V|^2, 0, 1)
 template <class RF = RowRuntime>
-__global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_kernel(BlasmDev d, const float2* __restrict__ B,
+__global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_inv_kernel(BlasmDev d, const float2* __restrict__ B,
                                                                      float2* __restrict__ V,
                                                                      float* __restrict__ pred) {
     extern __shared__ float2 sm[];
@@ -207,7 +211,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_kernel(BlasmDev
 // ---------------------------------------------------------------------------
 // K3b: gradient row embedded at the out_w centred columns -> forward FFT
 template <class RF = RowRuntime>
-__global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_fwd_adj_kernel(BlasmDev d, const float2* __restrict__ gV,
+__global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_fwd_adj_kernel(BlasmDev d, const float2* __restrict__ gV,
                                                                          const float* __restrict__ gpred,
                                                                          const float2* __restrict__ Vf,
                                                                          float2* __restrict__ Bt) {
@@ -291,7 +295,7 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_kernel(BlasmDev
 // K1b: inverse row FFT (first pass reads global), keep the input columns,
 // apply the amplitude-clamp adjoint against the splat field
 template <class RF = RowRuntime>
-__global__ void __launch_bounds__(kRowThreads, 3) blasm_rows_inv_adj_kernel(BlasmDev d, const float2* __restrict__ Ab,
+__global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_inv_adj_kernel(BlasmDev d, const float2* __restrict__ Ab,
                                                                          const float2* __restrict__ field,
                                                                          float2* __restrict__ gin) {
     extern __shared__ float2 sm[];
@@ -525,14 +529,14 @@ template <class RF>
 static void rows_forward(const BlasmDev& d, const float2* in, float2* A, cudaStream_t s) {
     const size_t rs = row_smem(d);
     CVQPG_SMEM_ATTR(blasm_rows_fwd_kernel<RF>, rs);
-    blasm_rows_fwd_kernel<RF><<<d.C * d.pH, kRowThreads, rs, s>>>(d, in, A);
+    blasm_rows_fwd_kernel<RF><<<d.C * d.pH, RF::kThreads, rs, s>>>(d, in, A);
 }
 
 template <class RF>
 static void rows_inverse(const BlasmDev& d, const float2* B, float2* out, float* pred, cudaStream_t s) {
     const size_t rs = row_smem(d);
     CVQPG_SMEM_ATTR(blasm_rows_inv_kernel<RF>, rs);
-    blasm_rows_inv_kernel<RF><<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, B, out, pred);
+    blasm_rows_inv_kernel<RF><<<d.P * d.C * d.out_h, RF::kThreads, rs, s>>>(d, B, out, pred);
 }
 
 template <class RF>
@@ -540,7 +544,7 @@ static void rows_forward_adjoint(const BlasmDev& d, const float2* grad_out, cons
                                  const float2* vfield, float2* B, cudaStream_t s) {
     const size_t rs = row_smem(d);
     CVQPG_SMEM_ATTR(blasm_rows_fwd_adj_kernel<RF>, rs);
-    blasm_rows_fwd_adj_kernel<RF><<<d.P * d.C * d.out_h, kRowThreads, rs, s>>>(d, grad_out, grad_pred, vfield, B);
+    blasm_rows_fwd_adj_kernel<RF><<<d.P * d.C * d.out_h, RF::kThreads, rs, s>>>(d, grad_out, grad_pred, vfield, B);
 }
 
 template <class RF>
@@ -549,7 +553,7 @@ static void rows_inverse_adjoint(const BlasmDev& d, const float2* A, const float
     const size_t rs = row_smem(d);
     const int in_h = d.input_mode == 0 ? d.H : d.pH;
     CVQPG_SMEM_ATTR(blasm_rows_inv_adj_kernel<RF>, rs);
-    blasm_rows_inv_adj_kernel<RF><<<d.C * in_h, kRowThreads, rs, s>>>(d, A, in_field, grad_in);
+    blasm_rows_inv_adj_kernel<RF><<<d.C * in_h, RF::kThreads, rs, s>>>(d, A, in_field, grad_in);
 }
 
 void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace, cudaStream_t s,
