@@ -659,6 +659,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
             }
             int nr = s_nr[e];
             int r = w & 15, x = ((w >> 4) & 15) + o, rem = (w >> 8) + 1 - o;
+            float fx = (float)(tx0 + x), fy = (float)(ty0 + r);  // pixel coordinates, advanced in float
 
             int g = point_list[b0 + e];
             float mx, my, i00, i01, i11, opac, curv, ar, kb, har, hcv, col[C], ph[C];
@@ -697,8 +698,8 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
             };
 
             for (int it = lo; it < hi; it++) {
-                const float dx = mx - (float)(tx0 + x);
-                const float dy = my - (float)(ty0 + r);
+                const float dx = mx - fx;
+                const float dy = my - fy;
                 const float mahal = dx * (i00 * dx + i01 * dy) + dy * (i01 * dx + i11 * dy);
                 if (mahal < kMahalCut) {
                     const float raw_power = -0.5f * mahal;
@@ -743,6 +744,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
                 }
                 // advance to the next active pixel of this entry, or to the next entry
                 x++;
+                fx += 1.0f;
                 if (--rem == 0) {
                     if (++k == nr) {
                         flush(e);
@@ -758,6 +760,8 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
                     r = w & 15;
                     x = (w >> 4) & 15;
                     rem = (w >> 8) + 1;
+                    fx = (float)(tx0 + x);
+                    fy = (float)(ty0 + r);
                 }
             }
             flush(e);  // no-op when the range ended on an entry boundary (sums already cleared)
