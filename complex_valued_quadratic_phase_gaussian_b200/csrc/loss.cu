@@ -58,7 +58,7 @@ __device__ __forceinline__ float ssim_w(int k) {
 }
 
 template <int NM>
-__global__ void __launch_bounds__(kLossThreads, 3) loss_kernel(LossDev L, const float* __restrict__ pred,
+__global__ void __launch_bounds__(kLossThreads, NM == 3 ? 4 : 3) loss_kernel(LossDev L, const float* __restrict__ pred,
                                                                 const float* __restrict__ target,
                                                                 const uint8_t* __restrict__ depth_plane,
                                                                 const float* __restrict__ noise_scale,
@@ -84,13 +84,30 @@ __global__ void __launch_bounds__(kLossThreads, 3) loss_kernel(LossDev L, const 
     const float* Y = target + plane_off;
     const int tid = threadIdx.x;
 
-    // 1. stage the 52x52 block (zeros outside the image; never used by valid map entries)
-    for (int i = tid; i < kLH * kLH; i += kLossThreads) {
-        const int r = i / kLH, q = i - r * kLH;
-        const int y = y0 - 10 + r, x = x0 - 10 + q;
-        const bool in = (unsigned)y < (unsigned)H && (unsigned)x < (unsigned)W;
-        sX[r * kSXLd + q] = in ? __ldg(&X[(size_t)y * W + x]) : 0.f;
-        sY[r * kSXLd + q] = in ? __ldg(&Y[(size_t)y * W + x]) : 0.f;
+    // 1. stage the 52x52 block (zeros outside the image; never used by valid map entries);
+    //    all loads of a thread are issued before its stores
+    {
+        constexpr int kStageIt = (kLH * kLH + kLossThreads - 1) / kLossThreads;
+        float vx[kStageIt], vy[kStageIt];
+#pragma unroll
+        for (int u = 0; u < kStageIt; u++) {
+            const int i = tid + u * kLossThreads;
+            const int r = i / kLH, q = i - r * kLH;
+            const int y = y0 - 10 + r, x = x0 - 10 + q;
+            const bool in = i < kLH * kLH && (unsigned)y < (unsigned)H && (unsigned)x < (unsigned)W;
+            const size_t e = in ? (size_t)y * W + x : 0;
+            vx[u] = in ? __ldg(&X[e]) : 0.f;
+            vy[u] = in ? __ldg(&Y[e]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < kStageIt; u++) {
+            const int i = tid + u * kLossThreads;
+            if (i < kLH * kLH) {
+                const int r = i / kLH, q = i - r * kLH;
+                sX[r * kSXLd + q] = vx[u];
+                sY[r * kSXLd + q] = vy[u];
+            }
+        }
     }
     __syncthreads();
 
@@ -258,13 +275,23 @@ __global__ void __launch_bounds__(kLossThreads, 3) loss_kernel(LossDev L, const 
                 z[2] = n4.z;
                 z[3] = n4.w;
             }
+            float xo[kTVSeg], to[kTVSeg];
+            uint8_t qo[kTVSeg];
+#pragma unroll
+            for (int o = 0; o < kTVSeg; o++) {  // loads first, so they are in flight together
+                const bool in = yb + o < H;
+                const size_t e = (size_t)(in ? yb + o : yb) * W + x;
+                xo[o] = __ldg(&X[e]);
+                to[o] = __ldg(&Y[e]);
+                qo[o] = __ldg(&depth_plane[e]);
+            }
 #pragma unroll
             for (int o = 0; o < kTVSeg; o++) {
                 const int y = yb + o;
                 if (y >= H) break;
                 const size_t e = (size_t)y * W + x;
-                const float xv = __ldg(&X[e]), tv = __ldg(&Y[e]);
-                const float m = (__ldg(&depth_plane[e]) == p) ? 1.f : 0.f;
+                const float xv = xo[o], tv = to[o];
+                const float m = (qo[o] == p) ? 1.f : 0.f;
                 const float nv = L.inject_noise ? tv + (z[o] * L.noise_ratio) * nscale : tv;
                 const float d0 = xv - tv, d1 = (xv * m - nv * m), d2 = (xv * nv - nv * nv);
                 l2_sum += L.w0 * d0 * d0 + L.w1 * d1 * d1 + L.w2 * d2 * d2;
