@@ -156,6 +156,17 @@ __global__ void __launch_bounds__(kLossThreads, NM == 3 ? 4 : 3) loss_kernel(Los
     float ssim_sum = 0.f;
     if (tid < kLM * (kLM / kVSeg)) {
         const int jj = tid % kLM, i0 = (tid / kLM) * kVSeg;
+        const int mj = x0 - 10 + jj;
+        const bool col_ok = (unsigned)mj < (unsigned)(W - 10);
+        float2 tmv[NM == 3 ? kVSeg : 1];
+        if (NM == 3) {  // the target moments of the 7 map positions, loads issued together
+#pragma unroll
+            for (int o = 0; o < (NM == 3 ? kVSeg : 1); o++) {
+                const int mi = y0 - 10 + i0 + o;
+                const bool ok = col_ok && (unsigned)mi < (unsigned)(H - 10);
+                tmv[o] = ok ? __ldg(&L.tmom[((size_t)pc * (H - 10) + mi) * (W - 10) + mj]) : make_float2(0.f, 0.f);
+            }
+        }
         float acc[NM][kVSeg];
 #pragma unroll
         for (int o = 0; o < kVSeg; o++)
@@ -175,8 +186,6 @@ __global__ void __launch_bounds__(kLossThreads, NM == 3 ? 4 : 3) loss_kernel(Los
                 for (int m = 0; m < NM; m++) acc[m][o] = fmaf(w, v[m], acc[m][o]);
             }
         }
-        const int mj = x0 - 10 + jj;
-        const bool col_ok = (unsigned)mj < (unsigned)(W - 10);
 #pragma unroll
         for (int o = 0; o < kVSeg; o++) {
             const int ii = i0 + o, mi = y0 - 10 + ii;
@@ -187,7 +196,7 @@ __global__ void __launch_bounds__(kLossThreads, NM == 3 ? 4 : 3) loss_kernel(Los
                     mu1 = acc[0][o], mu2 = acc[1 % NM][o], exx = acc[2 % NM][o], eyy = acc[3 % NM][o];
                     exy = acc[4 % NM][o];
                 } else {
-                    const float2 tm = __ldg(&L.tmom[((size_t)pc * (H - 10) + mi) * (W - 10) + mj]);
+                    const float2 tm = tmv[NM == 3 ? o : 0];
                     mu1 = acc[0][o], exx = acc[1][o], exy = acc[2][o], mu2 = tm.x, eyy = tm.y;
                 }
                 const float s11 = exx - mu1 * mu1, s22 = eyy - mu2 * mu2, s12 = exy - mu1 * mu2;
