@@ -572,6 +572,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     __shared__ uint16_t s_rows[kBwdBatch][kTile];
     __shared__ uint8_t s_nr[kBwdBatch];
     __shared__ int s_off[kBwdBatch + 1];
+    __shared__ int s_gid[kBwdBatch];  // Gaussian index of each entry of the batch
     __shared__ float s_acc[NA][kBwdBatch];
     __shared__ int s_wsum[kWarps];
     static_assert(kBwdBatch % kBwdThreads == 0, "whole entries per thread");
@@ -581,13 +582,24 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     if (range.y <= range.x) return;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     const int tx0 = (tile % gx) * kTile, ty0 = (tile / gx) * kTile;
-    for (int p = t; p < kTilePixels; p += kBwdThreads) {
-        const int px = tx0 + (p & 15), py = ty0 + (p >> 4);
-        const bool inside = px < W && py < H;
+    {  // the tile's dL/dU, all loads of a thread issued before its stores
+        constexpr int kIt = kTilePixels / kBwdThreads;
+        float2 gv[kIt][C];
 #pragma unroll
-        for (int c = 0; c < C; c++)
-            s_g[c][p] = inside ? grad[(size_t)c * H * W + (size_t)py * W + px] : make_float2(0.0f, 0.0f);
+        for (int u = 0; u < kIt; u++) {
+            const int p = t + u * kBwdThreads;
+            const int px = tx0 + (p & 15), py = ty0 + (p >> 4);
+            const bool inside = px < W && py < H;
+            const size_t e = inside ? (size_t)py * W + px : 0;
+#pragma unroll
+            for (int c = 0; c < C; c++) gv[u][c] = inside ? grad[(size_t)c * H * W + e] : make_float2(0.0f, 0.0f);
+        }
+#pragma unroll
+        for (int u = 0; u < kIt; u++)
+#pragma unroll
+            for (int c = 0; c < C; c++) s_g[c][t + u * kBwdThreads] = gv[u][c];
     }
+    static_assert(kTilePixels % kBwdThreads == 0, "whole pixel rounds");
     const int xmax = min(kTile, W - tx0), ymax = min(kTile, H - ty0);
 
     float kc[C];
@@ -597,16 +609,25 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     for (int b0 = range.x; b0 < range.y; b0 += kBwdBatch) {
         const int nb = min(kBwdBatch, range.y - b0);
         // 1. spans and active counts; thread t owns entries kPer*t .. kPer*t + kPer-1
-        int cnt[kPer];
+        int cnt[kPer], gid[kPer];
+        float4 r0s[kPer];
+        float i11s[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; u++) gid[u] = kPer * t + u < nb ? point_list[b0 + kPer * t + u] : 0;
+#pragma unroll
+        for (int u = 0; u < kPer; u++) {
+            r0s[u] = __ldg(&rec[(size_t)gid[u] * 4 + 0]);
+            i11s[u] = __ldg(&rec[(size_t)gid[u] * 4 + 1]).x;
+        }
 #pragma unroll
         for (int u = 0; u < kPer; u++) {
             const int e = kPer * t + u;
             cnt[u] = 0;
             int nr = 0;
+            s_gid[e] = gid[u];
             if (e < nb) {
-                const int g = point_list[b0 + e];
-                const float4 r0 = __ldg(&rec[(size_t)g * 4 + 0]);
-                const float i11 = __ldg(&rec[(size_t)g * 4 + 1]).x;
+                const float4 r0 = r0s[u];
+                const float i11 = i11s[u];
                 for (int yy = 0; yy < ymax; yy++) {
                     int x0, n;
                     cut_row_span(r0.x, r0.y, r0.z, r0.w, i11, (float)(ty0 + yy), tx0, xmax, &x0, &n);
@@ -661,7 +682,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
             int r = w & 15, x = ((w >> 4) & 15) + o, rem = (w >> 8) + 1 - o;
             float fx = (float)(tx0 + x), fy = (float)(ty0 + r);  // pixel coordinates, advanced in float
 
-            int g = point_list[b0 + e];
+            int g = s_gid[e];
             float mx, my, i00, i01, i11, opac, curv, ar, kb, har, hcv, col[C], ph[C];
             auto load = [&](int gg) {
                 const float4 r0 = __ldg(&rec[(size_t)gg * 4 + 0]);
@@ -751,7 +772,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
                         if (it + 1 >= hi) break;
                         e++;
                         while (e + 1 < nb && s_off[e + 1] == s_off[e]) e++;  // skip entries with no active pixel
-                        g = point_list[b0 + e];
+                        g = s_gid[e];
                         load(g);
                         nr = s_nr[e];
                         k = 0;
@@ -769,7 +790,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
         __syncthreads();
         // 4. one global atomic per parameter per (Gaussian, tile)
         for (int e = t; e < nb; e += kBwdThreads) {
-            const int g = point_list[b0 + e];
+            const int g = s_gid[e];
             float v[NA];
 #pragma unroll
             for (int q = 0; q < NA; q++) v[q] = s_acc[q][e];
