@@ -77,7 +77,7 @@ bool make_fft_plan(int n, FftPlan* plan, int order) {
 // handled by neighbouring CTAs at the same time, so the 32-byte sectors are
 // completed in L2.
 // ---------------------------------------------------------------------------
-// Row FFT policies: RowRuntime runs the plan read at run time; RowCT<N, R...>
+// Row FFT policies: RowRuntime runs the plan read at run time; RowCT<NT, MI, MO, N, R...>
 // the plan fixed at compile time (CtFft), for the row length of the 1080p fit.
 struct RowRuntime {
     static constexpr int kThreads = kRowThreads;
@@ -87,22 +87,28 @@ struct RowRuntime {
     }
 };
 
-template <int NT, int N, int... R>
+// MI / MO: the row's input is zero outside its middle half / only the middle
+// half of the output is kept (2x zero padding; the crops are at most the padded
+// width), so the first / last radix-16 pass is pruned (ct_pass MID_IN / MID_OUT).
+template <int NT, bool MI, bool MO, int N, int... R>
 struct RowCT {
     static constexpr int kThreads = NT;
     static constexpr int kPasses = (int)sizeof...(R);
     template <bool INV, typename Src>
     __device__ static __forceinline__ float2* run(Src src, float2* b0, float2* b1, int, const BlasmDev& d) {
         float2* res = (kPasses % 2 == 1) ? b0 : b1;  // the buffer the last pass does not read
-        CtFft<5, NT, N, INV, 1, R...>::run(ElemLoadF<Src>{src}, SmemStoreF<5>{res}, b0, b1, d.row.tw);
+        CtFft<5, NT, N, INV, 1, MI, MO, R...>::run(ElemLoadF<Src>{src}, SmemStoreF<5>{res}, b0, b1, d.row.tw);
         return res;
     }
 };
 
-// The 1080p fit's rows: 2 x 2240 = 4480 = 16 x 8 x 5 x 7 (the default radix order);
-// 320 threads = 280, 560, 896, 640 butterflies in 1, 2, 3, 2 rounds.
+// The 1080p fit's rows: 2 x 2240 = 4480 = 16 x 8 x 5 x 7 (forward kernels, the
+// pruned radix 16 first) and 8 x 5 x 7 x 16 (inverse kernels, radix 16 last);
+// 320 threads = 280, 560, 896, 640 butterflies in 1, 2, 3, 2 rounds. The run-time
+// plan must be the default one (its twiddle table serves both orders).
 constexpr int kRow4480Threads = 320;
-using Row4480 = RowCT<kRow4480Threads, 4480, 16, 8, 5, 7>;
+using Row4480F = RowCT<kRow4480Threads, true, false, 4480, 16, 8, 5, 7>;
+using Row4480I = RowCT<kRow4480Threads, false, true, 4480, 8, 5, 7, 16>;
 static bool row_is_4480(const BlasmDev& d) {
     const unsigned long long code = 16ull | (8ull << 5) | (5ull << 10) | (7ull << 15);
     return d.NW == 4480 && d.row.npass == 4 && d.row.code == code;
@@ -561,11 +567,11 @@ void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred
     float2 *A, *B;
     carve(d, workspace, &A, &B);
     const bool ct = row_is_4480(d);
-    if (ct) rows_forward<Row4480>(d, in, A, s); else rows_forward<RowRuntime>(d, in, A, s);
+    if (ct) rows_forward<Row4480F>(d, in, A, s); else rows_forward<RowRuntime>(d, in, A, s);
     if (marks) marks->mark(s);
     launch_columns(false, d, A, B, s);
     if (marks) marks->mark(s);
-    if (ct) rows_inverse<Row4480>(d, B, out, pred, s); else rows_inverse<RowRuntime>(d, B, out, pred, s);
+    if (ct) rows_inverse<Row4480I>(d, B, out, pred, s); else rows_inverse<RowRuntime>(d, B, out, pred, s);
     if (marks) marks->mark(s);
 }
 
@@ -575,13 +581,13 @@ void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* gra
     carve(d, workspace, &A, &B);
     const bool ct = row_is_4480(d);
     if (ct)
-        rows_forward_adjoint<Row4480>(d, grad_out, grad_pred, vfield, B, s);
+        rows_forward_adjoint<Row4480F>(d, grad_out, grad_pred, vfield, B, s);
     else
         rows_forward_adjoint<RowRuntime>(d, grad_out, grad_pred, vfield, B, s);
     if (marks) marks->mark(s);
     launch_columns(true, d, B, A, s);
     if (marks) marks->mark(s);
-    if (ct) rows_inverse_adjoint<Row4480>(d, A, in_field, grad_in, s);
+    if (ct) rows_inverse_adjoint<Row4480I>(d, A, in_field, grad_in, s);
     else rows_inverse_adjoint<RowRuntime>(d, A, in_field, grad_in, s);
     if (marks) marks->mark(s);
 }

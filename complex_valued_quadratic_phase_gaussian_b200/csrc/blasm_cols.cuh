@@ -117,22 +117,28 @@ struct HeadRuntime {
     }
 };
 
+// The BLASM columns are zero-padded 2x: a forward column FFT's input is zero
+// outside rows [N/4, 3N/4), and only rows inside [N/4, 3N/4) of an inverse one
+// are kept (the output crop is at most the padded height). So the first forward
+// pass loads 8 of its 16 inputs and the last inverse pass forms 8 of its 16
+// outputs (ct_pass MID_IN / MID_OUT).
 template <int N, int RA, int RB>
 struct HeadCT2 {
     static constexpr int kN = N;
+    static_assert(RA == 16 && RB == 16, "the middle-half passes are radix 16");
     template <typename Src>
     __device__ static __forceinline__ float2* forward(Src src, float2* b0, float2* b1, int, int, const ColSplit&,
                                                       const float2* tw) {
-        CtFft<kColPad, kColThreads, N, false, 1, RA, RB>::run(ElemLoadF<Src>{src}, SmemStoreF<kColPad>{b1}, b0, b1,
-                                                              tw);
+        ct_pass<kColThreads, N, RA, 1, false, true, false>(ElemLoadF<Src>{src}, SmemStoreF<kColPad>{b0}, tw);
+        ct_pass<kColThreads, N, RB, RA, false>(SmemLoadF<kColPad>{b0}, SmemStoreF<kColPad>{b1}, tw);
         return b1;
     }
     template <typename Sink>
     __device__ static __forceinline__ void inverse(Sink sink, float2* b0, float2* b1, int, int, int,
                                                    const ColSplit&, const float2* tw) {
         constexpr int RL = N / (RA * RB);
-        CtFft<kColPad, kColThreads, N, true, RL, RA, RB>::run(SmemLoadF<kColPad>{b0}, ElemStoreF<Sink>{sink}, b1,
-                                                               b0, tw);
+        ct_pass<kColThreads, N, RA, RL, true>(SmemLoadF<kColPad>{b0}, SmemStoreF<kColPad>{b1}, tw);
+        ct_pass<kColThreads, N, RB, RL * RA, true, false, true>(SmemLoadF<kColPad>{b1}, ElemStoreF<Sink>{sink}, tw);
     }
 };
 

@@ -56,6 +56,54 @@ __device__ __forceinline__ void dft4(float2& x0, float2& x1, float2& x2, float2&
     x3 = csub(t1, r);
 }
 
+// Second half of the 4 x 4 DFT-16 (twiddle W16^(n2 k1), row DFTs over n2,
+// transpose). MID_OUT: only the outputs 4..11 are formed (rows k2 = 1, 2 of
+// each row DFT); the others are left undefined.
+template <bool MID_OUT = false>
+__device__ __forceinline__ void dft16_twiddle_rows(float2 (&v)[16], bool inv) {
+#pragma unroll
+    for (int n2 = 1; n2 < 4; n2++)
+#pragma unroll
+        for (int k1 = 1; k1 < 4; k1++) {
+            const int q = (n2 * k1) & 15;
+            const float2 w = make_float2(DftTab<16>::c(q), inv ? DftTab<16>::s(q) : -DftTab<16>::s(q));
+            v[4 * k1 + n2] = cmul(v[4 * k1 + n2], w);
+        }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+        if constexpr (!MID_OUT) {
+            dft4(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3], inv);
+        } else {  // the k2 = 1, 2 outputs of dft4 only
+            const float2 x0 = v[4 * k1], x1 = v[4 * k1 + 1], x2 = v[4 * k1 + 2], x3 = v[4 * k1 + 3];
+            const float2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = csub(x1, x3);
+            v[4 * k1 + 1] = cadd(t1, mul_i(t3, !inv));
+            v[4 * k1 + 2] = csub(t0, t2);
+        }
+    }
+    float2 x[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) x[k1 + 4 * k2] = v[4 * k1 + k2];
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = x[k];
+}
+
+// DFT-16 whose inputs other than 4..11 are zero: the column DFTs over n1 have
+// x0 = x3 = 0 (same values as dft<16> on the zero-filled input).
+__device__ __forceinline__ void dft16_mid_in(float2 (&v)[16], bool inv) {
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+        const float2 a = v[4 + n2], b = v[8 + n2];
+        const float2 r = mul_i(a, !inv);
+        v[n2] = cadd(b, a);
+        v[8 + n2] = csub(b, a);
+        v[4 + n2] = csub(r, b);
+        v[12 + n2] = make_float2(-b.x - r.x, -b.y - r.y);
+    }
+    dft16_twiddle_rows(v, inv);
+}
+
 template <int R>
 __device__ __forceinline__ void dft(float2 (&v)[R], bool inv) {
     if constexpr (R == 2) {
@@ -83,23 +131,7 @@ __device__ __forceinline__ void dft(float2 (&v)[R], bool inv) {
         // then the 4x4 transpose is a compile-time renaming of registers.
 #pragma unroll
         for (int n2 = 0; n2 < 4; n2++) dft4(v[n2], v[4 + n2], v[8 + n2], v[12 + n2], inv);
-#pragma unroll
-        for (int n2 = 1; n2 < 4; n2++)
-#pragma unroll
-            for (int k1 = 1; k1 < 4; k1++) {
-                const int q = (n2 * k1) & 15;
-                const float2 w = make_float2(DftTab<16>::c(q), inv ? DftTab<16>::s(q) : -DftTab<16>::s(q));
-                v[4 * k1 + n2] = cmul(v[4 * k1 + n2], w);
-            }
-#pragma unroll
-        for (int k1 = 0; k1 < 4; k1++) dft4(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3], inv);
-        float2 x[16];
-#pragma unroll
-        for (int k1 = 0; k1 < 4; k1++)
-#pragma unroll
-            for (int k2 = 0; k2 < 4; k2++) x[k1 + 4 * k2] = v[4 * k1 + k2];
-#pragma unroll
-        for (int k = 0; k < 16; k++) v[k] = x[k];
+        dft16_twiddle_rows(v, inv);
     } else {
         // odd R: X_k = x0 + sum_m (x_m + x_{R-m}) cos(2 pi m k/R) -/+ i (x_m - x_{R-m}) sin(2 pi m k/R);
         // the inputs are folded into a[], b[] first, then the outputs overwrite v.
@@ -343,21 +375,53 @@ struct ElemStoreF {  // element writes through sink(0, a, v)
     }
 };
 
-template <int NT, int N, int R, int NS, bool INV, typename Load, typename Store>
+// MID_IN (first pass, NS = 1): the input is zero outside its middle half
+// [N/4, 3N/4), i.e. outside r in [R/4, 3R/4); only those elements are loaded.
+// MID_OUT (last pass, NS = N/R): only the middle half of the output is used;
+// only r in [R/4, 3R/4) is formed and stored. Both for R = 16.
+template <int NT, int N, int R, int NS, bool INV, bool MID_IN = false, bool MID_OUT = false, typename Load,
+          typename Store>
 __device__ __forceinline__ void ct_pass(const Load& load, const Store& store, const float2* tw) {
+    static_assert(!(MID_IN || MID_OUT) || R == 16, "middle-half pruning is written for radix 16");
+    static_assert(!MID_IN || NS == 1, "input pruning applies to the first pass");
+    static_assert(!MID_OUT || NS * R == N, "output pruning applies to the last pass");
     constexpr int nb = N / R;
     constexpr int stride = N / (NS * R);
     for (int j = threadIdx.x; j < nb; j += NT) {
         const int q = j / NS, k = j - q * NS;
         float2 v[R];
-        load.template get<N, R>(j, v);
+        if constexpr (MID_IN) {
+            float2 m[R / 2];
+            load.template get<N / 2, R / 2>(j + N / 4, m);  // m[i] = x[j + N/4 + i N/R]
+#pragma unroll
+            for (int i = 0; i < R / 2; i++) v[R / 4 + i] = m[i];
+#pragma unroll
+            for (int i = 0; i < R / 4; i++) v[i] = v[3 * R / 4 + i] = make_float2(0.f, 0.f);
+        } else {
+            load.template get<N, R>(j, v);
+        }
         if constexpr (NS > 1) {
             float2 w = tw[k * stride];
             if (INV) w.y = -w.y;
             apply_twiddles<R>(v, w);
         }
-        dft<R>(v, INV);
-        store.template put<NS, R>(q * NS * R + k, v);
+        if constexpr (MID_IN) {
+            dft16_mid_in(reinterpret_cast<float2(&)[16]>(v), INV);
+        } else if constexpr (MID_OUT) {
+#pragma unroll
+            for (int n2 = 0; n2 < 4; n2++) dft4(v[n2], v[4 + n2], v[8 + n2], v[12 + n2], INV);
+            dft16_twiddle_rows<true>(reinterpret_cast<float2(&)[16]>(v), INV);
+        } else {
+            dft<R>(v, INV);
+        }
+        if constexpr (MID_OUT) {
+            float2 m[R / 2];
+#pragma unroll
+            for (int i = 0; i < R / 2; i++) m[i] = v[R / 4 + i];
+            store.template put<NS, R / 2>(q * NS * R + k + (R / 4) * NS, m);
+        } else {
+            store.template put<NS, R>(q * NS * R + k, v);
+        }
     }
     __syncthreads();
 }
@@ -365,17 +429,18 @@ __device__ __forceinline__ void ct_pass(const Load& load, const Store& store, co
 // Passes R, Rest... of length N from stride NS: the first reads through `load`,
 // the intermediate ones ping-pong a -> b -> a ..., the last writes through `last`
 // (which must not be the buffer the last pass reads: buffer (passes - 2) % 2).
-template <int PS, int NT, int N, bool INV, int NS, int R, int... Rest>
+// MI / MO: middle-half pruning of the first / last pass (ct_pass MID_IN / MID_OUT).
+template <int PS, int NT, int N, bool INV, int NS, bool MI, bool MO, int R, int... Rest>
 struct CtFft {
     static constexpr int kPasses = 1 + (int)sizeof...(Rest);
     template <typename Load, typename Store>
     __device__ static __forceinline__ void run(const Load& load, const Store& last, float2* a, float2* b,
                                                const float2* tw) {
         if constexpr (sizeof...(Rest) == 0) {
-            ct_pass<NT, N, R, NS, INV>(load, last, tw);
+            ct_pass<NT, N, R, NS, INV, MI, MO>(load, last, tw);
         } else {
-            ct_pass<NT, N, R, NS, INV>(load, SmemStoreF<PS>{a}, tw);
-            CtFft<PS, NT, N, INV, NS * R, Rest...>::run(SmemLoadF<PS>{a}, last, b, a, tw);
+            ct_pass<NT, N, R, NS, INV, MI, false>(load, SmemStoreF<PS>{a}, tw);
+            CtFft<PS, NT, N, INV, NS * R, false, MO, Rest...>::run(SmemLoadF<PS>{a}, last, b, a, tw);
         }
     }
 };
