@@ -196,7 +196,7 @@ def kernels_per_fit_step(cfg):
     lists = ((cfg.W + 15) // 16) * ((cfg.H + 15) // 16)
     bits = max(1, math.ceil(math.log2(max(lists, 2))))
     passes = 1 if bits <= 8 else (bits + 7) // 8
-    binning = 1 + 3 + 1 + 4 * passes + 1
+    binning = 1 + 3 + 1 + 4 * passes + 1 + 1  # ... + ranges + tile order
     return 1 + binning + 1 + 3 + 2 + 1 + 3 + 1 + 1 + 1 + 1
 
 

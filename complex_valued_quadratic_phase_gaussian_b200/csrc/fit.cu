@@ -24,6 +24,7 @@ struct FitLayout {
     int32_t* point_list;
     int32_t* ranges;
     int32_t* pair_count;
+    int32_t* tile_order;  // longest-list-first launch order of the splat tiles
     float2* field;      // splat output U [C,H,W]
     float2* vfield;     // V [P,C,H,W]
     float* pred;        // clamp(|V|^2) [P,C,H,W]
@@ -97,6 +98,7 @@ static int fit_layout(const cvqpg_fit_params* q, void* base, size_t cap, FitLayo
     L->point_list = cv.take<int32_t>(q->pair_capacity > 0 ? q->pair_capacity : 1);
     L->ranges = cv.take<int32_t>((size_t)2 * bin_rule_lists(rule));
     L->pair_count = cv.take<int32_t>(2);
+    L->tile_order = cv.take<int32_t>((size_t)((W + kTile - 1) / kTile) * ((H + kTile - 1) / kTile));
     L->field = cv.take<float2>((size_t)C * H * W);
     L->vfield = cv.take<float2>((size_t)P * C * H * W);
     L->pred = cv.take<float>((size_t)P * C * H * W);
@@ -184,10 +186,11 @@ static void run_forward(const cvqpg_fit_params* q, const FitLayout& L, const Bla
     launch_preprocess_forward(C, P, raw, L.records, L.radii, L.radius3, L.bin.tiles_touched, rule, s);
     if (marks) marks->mark(s);
     launch_binning(rule, L.records, L.bin, L.point_list, L.ranges, L.pair_count, s);
+    launch_tile_order(rule, L.ranges, L.tile_order, s);
     if (marks) marks->mark(s);
     const float dxy2 = (float)(q->pixel_pitch * q->pixel_pitch);
     launch_splat_forward(C, rule, L.ranges, L.point_list, L.records, L.kvec, dxy2, L.field, s,
-                         (q->cull_mode & CVQPG_PHASE_ISO) != 0);
+                         (q->cull_mode & CVQPG_PHASE_ISO) != 0, L.tile_order);
     if (marks) marks->mark(s);
     blasm_forward(bd, L.field, L.vfield, L.pred, L.blasm_ws, s, marks);
     launch_loss(ld, L.pred, targets, depth_plane, target_range, iteration, L.gpred, L.loss_partials, L.loss_out, s);
@@ -268,7 +271,7 @@ static int fit_step_impl(const cvqpg_fit_params* q, float* params, float* grads,
     const BinRule rule = make_bin_rule(q->cull_mode & ~CVQPG_PHASE_ISO, q->width, q->height, L.radii, L.radius3);
     const float dxy2 = (float)(q->pixel_pitch * q->pixel_pitch);
     launch_splat_backward(C, rule, L.ranges, L.point_list, L.records, L.kvec, dxy2, L.gfield, out, s,
-                          (q->cull_mode & CVQPG_PHASE_ISO) != 0);
+                          (q->cull_mode & CVQPG_PHASE_ISO) != 0, L.tile_order);
     if (marks) marks->mark(s);
     // preprocessing adjoint + nan_to_num + norm partials
     SplatGradsIn gin{out.d_means, out.d_inv, out.d_col, out.d_ph, out.d_op, out.d_cv, out.d_ar};

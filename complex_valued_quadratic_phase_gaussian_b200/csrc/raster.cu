@@ -411,6 +411,59 @@ __device__ __forceinline__ int list_of_tile(const BinRule& R, int tx, int ty) {
     return 0;
 }
 
+// Launch order of the 16-px splat tiles, longest list first (a counting sort on
+// list length / 4, lengths above 4095 sharing the first bucket): the block
+// scheduler then hands the heaviest tiles out first and the last wave holds
+// short ones (longest-processing-time-first list scheduling). One CTA.
+constexpr int kOrderThreads = 1024;
+__global__ void __launch_bounds__(kOrderThreads) tile_order_kernel(BinRule rule, const int32_t* __restrict__ ranges,
+                                                                 int gx, int ntiles, int32_t* __restrict__ order) {
+    __shared__ int cnt[kOrderThreads];
+    __shared__ int wsum[kOrderThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int2* r2 = reinterpret_cast<const int2*>(ranges);
+    cnt[t] = 0;
+    __syncthreads();
+    for (int i = t; i < ntiles; i += kOrderThreads) {
+        const int2 r = r2[list_of_tile(rule, i % gx, i / gx)];
+        atomicAdd(&cnt[kOrderThreads - 1 - min(max(r.y - r.x, 0), 4 * kOrderThreads - 1) / 4], 1);
+    }
+    __syncthreads();
+    const int v = cnt[t];
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const int x = wsum[lane];
+        int ix = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, ix, o);
+            if (lane >= o) ix += y;
+        }
+        wsum[lane] = ix - x;
+    }
+    __syncthreads();
+    cnt[t] = wsum[w] + incl - v;
+    __syncthreads();
+    for (int i = t; i < ntiles; i += kOrderThreads) {
+        const int2 r = r2[list_of_tile(rule, i % gx, i / gx)];
+        const int pos = atomicAdd(&cnt[kOrderThreads - 1 - min(max(r.y - r.x, 0), 4 * kOrderThreads - 1) / 4], 1);
+        order[pos] = i;
+    }
+}
+
+void launch_tile_order(const BinRule& rule, const int32_t* ranges, int32_t* order, cudaStream_t stream) {
+    const int gx = (rule.width + kTile - 1) / kTile, gy = (rule.height + kTile - 1) / kTile;
+    tile_order_kernel<<<1, kOrderThreads, 0, stream>>>(rule, ranges, gx, gx * gy, order);
+}
+
+
 // ---------------------------------------------------------------------------
 // splat forward: one CTA per 16x16 tile, one pixel per thread, each warp an
 // 8x4 pixel block; Gaussian batches of 256 records staged in shared memory.
@@ -419,10 +472,10 @@ template <int C, bool ISO>
 __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
     BinRule rule, const int32_t* __restrict__ ranges, const int32_t* __restrict__ point_list,
     const float4* __restrict__ rec, const float* __restrict__ k, float dxy2, float2* __restrict__ out, int W, int H,
-    int gx) {
+    int gx, const int32_t* __restrict__ order) {
     constexpr int NV = (8 + 2 * C + 3) / 4;  // float4 words used per record
     __shared__ float4 s_rec[kTilePixels][NV];
-    const int tile = blockIdx.x;
+    const int tile = order ? order[blockIdx.x] : blockIdx.x;
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int px = (tile % gx) * kTile + (w & 1) * 8 + (lane & 7);
     const int py = (tile / gx) * kTile + (w >> 1) * 4 + (lane >> 3);
@@ -489,7 +542,7 @@ __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
 
 void launch_splat_forward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
                           const float* records, const float* k, float dxy2, float2* out, cudaStream_t stream,
-                          bool iso) {
+                          bool iso, const int32_t* tile_order) {
     const int width = rule.width, height = rule.height;
     const int gx = (width + kTile - 1) / kTile, gy = (height + kTile - 1) / kTile;
     const float4* rec = reinterpret_cast<const float4*>(records);
@@ -497,17 +550,17 @@ void launch_splat_forward(int channels, const BinRule& rule, const int32_t* rang
     if (channels == 1) {
         if (iso)
             splat_forward_kernel<1, true><<<grid, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                            out, width, height, gx);
+                                                                            out, width, height, gx, tile_order);
         else
             splat_forward_kernel<1, false><<<grid, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                             out, width, height, gx);
+                                                                             out, width, height, gx, tile_order);
     } else {
         if (iso)
             splat_forward_kernel<3, true><<<grid, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                            out, width, height, gx);
+                                                                            out, width, height, gx, tile_order);
         else
             splat_forward_kernel<3, false><<<grid, kTilePixels, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                             out, width, height, gx);
+                                                                             out, width, height, gx, tile_order);
     }
 }
 
@@ -563,7 +616,7 @@ template <int C, bool ISO>
 __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     BinRule rule, const int32_t* __restrict__ ranges, const int32_t* __restrict__ point_list,
     const float4* __restrict__ rec, const float* __restrict__ k, float dxy2, const float2* __restrict__ grad, int W,
-    int H, int gx, SplatGrads out) {
+    int H, int gx, SplatGrads out, const int32_t* __restrict__ order) {
     constexpr int NA = 8 + 2 * C;  // dmx dmy d00 d01 d11 dop dcv dar dcol[C] dph[C]
     constexpr int kWarps = kBwdThreads / 32;
     constexpr int kPer = kBwdBatch / kBwdThreads;  // entries per thread in the span pass
@@ -577,7 +630,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     __shared__ int s_wsum[kWarps];
     static_assert(kBwdBatch % kBwdThreads == 0, "whole entries per thread");
 
-    const int tile = blockIdx.x;
+    const int tile = order ? order[blockIdx.x] : blockIdx.x;
     const int2 range = reinterpret_cast<const int2*>(ranges)[list_of_tile(rule, tile % gx, tile / gx)];
     if (range.y <= range.x) return;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
@@ -814,7 +867,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
 
 void launch_splat_backward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
                            const float* records, const float* k, float dxy2, const float2* grad,
-                           const SplatGrads& out, cudaStream_t stream, bool iso) {
+                           const SplatGrads& out, cudaStream_t stream, bool iso, const int32_t* tile_order) {
     const int width = rule.width, height = rule.height;
     const int gx = (width + kTile - 1) / kTile, gy = (height + kTile - 1) / kTile;
     const float4* rec = reinterpret_cast<const float4*>(records);
@@ -822,17 +875,17 @@ void launch_splat_backward(int channels, const BinRule& rule, const int32_t* ran
     if (channels == 1) {
         if (iso)
             splat_backward_kernel<1, true><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                             grad, width, height, gx, out);
+                                                                             grad, width, height, gx, out, tile_order);
         else
             splat_backward_kernel<1, false><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                              grad, width, height, gx, out);
+                                                                              grad, width, height, gx, out, tile_order);
     } else {
         if (iso)
             splat_backward_kernel<3, true><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                             grad, width, height, gx, out);
+                                                                             grad, width, height, gx, out, tile_order);
         else
             splat_backward_kernel<3, false><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                              grad, width, height, gx, out);
+                                                                              grad, width, height, gx, out, tile_order);
     }
 }
 

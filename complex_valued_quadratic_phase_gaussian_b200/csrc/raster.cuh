@@ -67,8 +67,13 @@ void launch_tile_count(const BinRule& rule, const float* records, int n, uint32_
 void launch_binning(const BinRule& rule, const float* records, const BinWorkspace& ws, int32_t* point_list,
                     int32_t* ranges, int32_t* pair_count, cudaStream_t stream);
 
+// tile_order (optional, launch_tile_order): CTA i renders tile tile_order[i].
 void launch_splat_forward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
-                          const float* records, const float* k, float dxy2, float2* out, cudaStream_t stream, bool iso = false);
+                          const float* records, const float* k, float dxy2, float2* out, cudaStream_t stream,
+                          bool iso = false, const int32_t* tile_order = nullptr);
+
+// Longest-list-first launch order of the 16-px tiles ([tiles] int32) from the ranges.
+void launch_tile_order(const BinRule& rule, const int32_t* ranges, int32_t* order, cudaStream_t stream);
 
 // Gradient outputs in the reference SoA layout; they are accumulated with
 // atomics and must be zeroed beforehand.
@@ -84,7 +89,8 @@ struct SplatGrads {
 
 void launch_splat_backward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
                            const float* records, const float* k, float dxy2, const float2* grad,
-                           const SplatGrads& out, cudaStream_t stream, bool iso = false);
+                           const SplatGrads& out, cudaStream_t stream, bool iso = false,
+                           const int32_t* tile_order = nullptr);
 
 // Tile rectangle of a Gaussian, written with the exact float operation order
 // of the reference getRect (cuda/forward.cu:8-13) so that the per-tile lists
