@@ -776,8 +776,9 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
                 const float dy = my - fy;
                 const float mahal = dx * (i00 * dx + i01 * dy) + dy * (i01 * dx + i11 * dy);
                 if (mahal < kMahalCut) {
-                    const float raw_power = -0.5f * mahal;
-                    const float G = __expf(fmaxf(raw_power, -50.0f));
+                    // mahal < 40 here, so the forward's clamp of the exponent at -50 never applies
+                    // (and its derivative factor is -1/2)
+                    const float G = __expf(-0.5f * mahal);
                     const float alpha = opac * G;
                     const float d2 = dx * dx + dy * dy;
                     const float base = ISO ? 0.5f * curv * d2 * dxy2 : 0.5f * curv * mahal * ar * dxy2;
@@ -796,7 +797,7 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
                         S_alpha = fmaf(col[c], proj_c, S_alpha);
                         S_base = fmaf(kc[c], aph, S_base);
                     }
-                    const float dpow = (raw_power >= -50.0f) ? -0.5f : 0.0f;
+                    const float dpow = -0.5f;
                     float dmahal;
                     if (ISO) {
                         // the phase reaches the means directly: dbase/dmu = c dxy2 (mu - r)
