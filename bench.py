@@ -197,7 +197,7 @@ def kernels_per_fit_step(cfg):
     bits = max(1, math.ceil(math.log2(max(lists, 2))))
     passes = 1 if bits <= 8 else (bits + 7) // 8
     binning = 1 + 3 + 1 + 4 * passes + 1 + 1  # ... + ranges + tile order
-    return 1 + binning + 1 + 3 + 2 + 1 + 3 + 1 + 1 + 1 + 1
+    return 1 + binning + 1 + 3 + 2 + 1 + 3 + 1 + 1 + 2 + 1  # ... preprocess adjoint, Adan scalars + step, record
 
 
 def build_scene(wl, seed, device, ours=False):

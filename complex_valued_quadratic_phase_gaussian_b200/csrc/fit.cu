@@ -33,6 +33,7 @@ struct FitLayout {
     float2* gfield;     // dL/dU [C,H,W]
     float* splat_grads; // SoA (8 + 2C) N
     float* norm_partials;
+    float* adan_scalars;  // clip factor and step sizes of the current step
     float* loss_partials;
     float* loss_out;    // 1 + 3P
     size_t total;
@@ -110,6 +111,7 @@ static int fit_layout(const cvqpg_fit_params* q, void* base, size_t cap, FitLayo
     L->gfield = cv.take<float2>((size_t)C * H * W);
     L->splat_grads = cv.take<float>((size_t)(8 + 2 * C) * n1);
     L->norm_partials = cv.take<float>(preprocess_backward_blocks(N));
+    L->adan_scalars = cv.take<float>(kAdanScalars);
     L->loss_partials = cv.take<float>(loss_partials_floats(*ld));
     L->loss_out = cv.take<float>(1 + 3 * P);
     L->total = cv.off + 256;
@@ -310,6 +312,7 @@ static int fit_step_impl(const cvqpg_fit_params* q, float* params, float* grads,
     A.max_grad_norm = q->max_grad_norm;
     A.norm_partials = L.norm_partials;
     A.num_partials = preprocess_backward_blocks(N);
+    A.scalars = L.adan_scalars;
     if (N > 0) launch_adan(A, iteration, s);
     if (marks) marks->mark(s);
     record_step_kernel<<<1, 32, 0, s>>>(L.loss_out, 0, L.pair_count, nullptr, 1, nullptr, iteration, 1);

@@ -17,48 +17,56 @@
 
 namespace cvqpg {
 
-__global__ void __launch_bounds__(256) adan_kernel(AdanDev A, const int32_t* __restrict__ iteration) {
-    const int t = blockIdx.y;
-    if (A.frozen_always[t]) return;
+// The step's scalars, once per launch (one warp): the clip_grad_norm_ factor
+// from the norm partials (fixed-order double sum) and, per tensor t at
+// scalars[8 + 8 t]: active, fresh (state created now), step size, step size of
+// the difference term, sqrt(bias correction 3), lr * weight decay.
+__global__ void adan_scalars_kernel(AdanDev A, const int32_t* __restrict__ iteration) {
+    const int lane = threadIdx.x;
+    double s = 0.0;
+    for (int k = lane; k < A.num_partials; k += 32) s += (double)A.norm_partials[k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     const int it = iteration ? iteration[0] : 0;
-    if (it < A.first_iter[t]) return;  // no gradient yet (frozen during warm-up)
+    if (lane == 0) {
+        float clip = 1.0f;
+        if (A.max_grad_norm > 0.0) {
+            const float total = (float)sqrt(s);
+            const float coef = (float)A.max_grad_norm / (total + 1e-6f);
+            clip = fminf(coef, 1.0f);
+        }
+        A.scalars[0] = clip;
+    }
+    if (lane < kParamTensors) {
+        const int t = lane;
+        const int grp = A.group[t];
+        const int step = it + 1;  // every group steps every iteration
+        const double lr = (grp == 0 && A.lr_table) ? A.lr_table[min(it, A.lr_table_len - 1)] : A.lr[grp];
+        const double bc1 = 1.0 - pow(A.beta1, (double)step);
+        const double bc2 = 1.0 - pow(A.beta2, (double)step);
+        const double bc3s = sqrt(1.0 - pow(A.beta3, (double)step));
+        float* o = A.scalars + 8 + 8 * t;
+        o[0] = (!A.frozen_always[t] && it >= A.first_iter[t]) ? 1.0f : 0.0f;  // frozen during warm-up: no gradient
+        o[1] = (it == A.first_iter[t]) ? 1.0f : 0.0f;  // state created now: zeros, neg_pre_grad = -grad*clip
+        o[2] = (float)(lr / bc1);
+        o[3] = (float)(lr * A.beta2 / bc2);
+        o[4] = (float)bc3s;
+        o[5] = (float)(lr * A.weight_decay);
+    }
+}
+
+__global__ void __launch_bounds__(256) adan_kernel(AdanDev A) {
+    const int t = blockIdx.y;
+    const float* sc = A.scalars + 8 + 8 * t;
+    if (sc[0] == 0.0f) return;
     const int n = A.numel[t];
     const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x * blockDim.x >= n) return;
-
-    // global gradient norm and clip coefficient (torch clip_grad_norm_)
-    __shared__ float s_clip;
-    if (threadIdx.x < 32) {
-        double s = 0.0;
-        for (int k = threadIdx.x; k < A.num_partials; k += 32) s += (double)A.norm_partials[k];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) {
-            float clip = 1.0f;
-            if (A.max_grad_norm > 0.0) {
-                const float total = (float)sqrt(s);
-                const float coef = (float)A.max_grad_norm / (total + 1e-6f);
-                clip = fminf(coef, 1.0f);
-            }
-            s_clip = clip;
-        }
-    }
-    __syncthreads();
-    const float clip = s_clip;
-
-    const int grp = A.group[t];
-    const int step = it + 1;  // every group steps every iteration
-    const double lr = (grp == 0 && A.lr_table) ? A.lr_table[min(it, A.lr_table_len - 1)] : A.lr[grp];
-    const double bc1 = 1.0 - pow(A.beta1, (double)step);
-    const double bc2 = 1.0 - pow(A.beta2, (double)step);
-    const double bc3s = sqrt(1.0 - pow(A.beta3, (double)step));
+    const float clip = A.scalars[0];
+    const bool fresh = sc[1] != 0.0f;
+    const float step_size = sc[2], step_size_diff = sc[3], bc3f = sc[4], wd = sc[5];
     const float b1 = (float)A.beta1, b2 = (float)A.beta2, b3 = (float)A.beta3;
     const float ob1 = (float)(1.0 - A.beta1), ob2 = (float)(1.0 - A.beta2), ob3 = (float)(1.0 - A.beta3);
-    const float step_size = (float)(lr / bc1);
-    const float step_size_diff = (float)(lr * A.beta2 / bc2);
-    const float bc3f = (float)bc3s;
     const float eps = (float)A.eps;
-    const float wd = (float)(lr * A.weight_decay);
-    const bool fresh = (it == A.first_iter[t]);  // state created now: zeros, neg_pre_grad = -grad*clip
 
     float* P = A.param[t];
     float* G = A.grad[t];
@@ -101,7 +109,8 @@ void launch_adan(const AdanDev& A, const int32_t* iteration, cudaStream_t s) {
     for (int t = 0; t < kParamTensors; t++) maxn = max(maxn, A.numel[t]);
     const unsigned bx = min(ceil_div(maxn, 256), 4096u);
     dim3 grid(bx, kParamTensors);
-    adan_kernel<<<grid, 256, 0, s>>>(A, iteration);
+    adan_scalars_kernel<<<1, 32, 0, s>>>(A, iteration);
+    adan_kernel<<<grid, 256, 0, s>>>(A);
 }
 
 }  // namespace cvqpg

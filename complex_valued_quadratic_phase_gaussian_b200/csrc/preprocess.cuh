@@ -78,7 +78,10 @@ struct AdanDev {
     double max_grad_norm;            // clip_grad_norm_ max_norm applied before the step (<= 0: none)
     const float* norm_partials;      // per-CTA sums of squares from the preprocess adjoint
     int num_partials;
+    float* scalars;                  // kAdanScalars floats of scratch: the step's clip factor and step sizes
 };
+
+constexpr int kAdanScalars = 8 + 8 * kParamTensors;
 
 void launch_adan(const AdanDev& A, const int32_t* iteration, cudaStream_t s);
 
