@@ -401,6 +401,9 @@ def run_ours(args, wl, dist, world, rank, local):
     ttp = None
     if rank == 0 and world == 1 and args.workload == "rgb1080" and not args.no_time_to_psnr:
         ttp = run_time_to_psnr()
+    batched = None
+    if rank == 0 and args.batched > 0:
+        batched = run_batched(args.batched, args.batched_iters, dev)
 
     if rank != 0:
         return None
@@ -435,7 +438,54 @@ def run_ours(args, wl, dist, world, rank, local):
         line["cpu_baseline"] = cpu
     if ttp is not None:
         line["time_to_psnr"] = ttp
+    if batched is not None:
+        line["batched"] = batched
     return line
+
+
+def run_batched(scenes, iters, dev):
+    """Batched-fitter workload: `scenes` RGB scenes, a third each at 512x512, 768x1024 and
+    1080x1920, with N proportional to the pixels (96k at 1080p), `iters` iterations each. The queue
+    runs once through the batched fitter (4 resident fits, one graph per iteration) and once one
+    fit at a time (1 slot), both timed with CUDA events on the stream that replays the graphs."""
+    from complex_valued_quadratic_phase_gaussian_b200 import scenes as S
+    from complex_valued_quadratic_phase_gaussian_b200.batch import BatchedFitter, FitJob
+    from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, synthetic_init
+    sizes = [(512, 512), (768, 1024), (1080, 1920)]
+    wl = WORKLOADS["rgb1080"]
+
+    def jobs():
+        out = []
+        for i in range(scenes):
+            H, W = sizes[i % 3]
+            img, depth = S.rgb_blobs(H, W, seed=100 + i)
+            t, q = S.multiplane_targets_device(img, depth, wl["P"], device=dev)
+            n = int(round(wl["N"] * H * W / (1080 * 1920)))
+            cfg = FitConfig(img_size=(W, H), num_gaussians=n, wavelengths=list(wl["wl"]), pixel_pitch=wl["pitch"],
+                            num_planes=wl["P"], d_val=wl["d_val"], volume_depth=wl["vd"], num_itrs=iters, seed=i)
+            out.append(FitJob(cfg, t, q, iters, init=synthetic_init(cfg, i), tag=(H, W, i)))
+        return out
+
+    res = {}
+    for name, slots in (("batched", 4), ("serial", 1)):
+        js = jobs()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = BatchedFitter(js, slots=slots, device=dev).run()
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        pix_it = sum(j.cfg.W * j.cfg.H * j.iters for j in js)
+        res[name] = {"seconds": round(sec, 3), "fit_iterations_per_s": round(scenes * iters / sec, 1),
+                     "megapixel_iterations_per_s": round(pix_it / sec / 1e6, 1), "slots": slots,
+                     "fits_done": len(out), "overflowed": sum(int(r.overflowed) for r in out)}
+        del out, js
+        torch.cuda.empty_cache()
+    res["speedup_batched_vs_serial"] = round(res["serial"]["seconds"] / res["batched"]["seconds"], 3)
+    res["workload"] = (f"{scenes} RGB scenes (512x512, 768x1024, 1080x1920 in turn; N = 96k x pixels / 1080p), "
+                       f"{iters} iterations each; fit set-up (targets' moments, workspaces) inside the timed region")
+    return res
 
 
 def run_time_to_psnr():
@@ -517,6 +567,9 @@ def main():
     ap.add_argument("--primitive", default="curv", choices=["curv", "flat"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched", type=int, default=0,
+                    help="also run the batched-fitter workload with this many scenes (48 = the c3 case)")
+    ap.add_argument("--batched-iters", type=int, default=500)
     ap.add_argument("--no-time-to-psnr", action="store_true",
                     help="skip the learned-vs-plain time-to-PSNR experiment (about a minute at N=1)")
     args = ap.parse_args()
