@@ -446,8 +446,9 @@ def run_ours(args, wl, dist, world, rank, local):
 def run_batched(scenes, iters, dev):
     """Batched-fitter workload: `scenes` RGB scenes, a third each at 512x512, 768x1024 and
     1080x1920, with N proportional to the pixels (96k at 1080p), `iters` iterations each. The queue
-    runs once through the batched fitter (4 resident fits, one graph per iteration) and once one
-    fit at a time (1 slot), both timed with CUDA events on the stream that replays the graphs."""
+    runs once through the batched fitter (one graph per iteration over the resident fits, admitted
+    while their pixels stay within two 1080p images, at most 16) and once one fit at a time (1 slot),
+    both timed with CUDA events on the stream that replays the graphs."""
     from complex_valued_quadratic_phase_gaussian_b200 import scenes as S
     from complex_valued_quadratic_phase_gaussian_b200.batch import BatchedFitter, FitJob
     from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, synthetic_init
@@ -467,18 +468,20 @@ def run_batched(scenes, iters, dev):
         return out
 
     res = {}
-    for name, slots in (("batched", 4), ("serial", 1)):
+    budget = int(2.05 * 1080 * 1920)
+    for name, slots in (("batched", 16), ("serial", 1)):
         js = jobs()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        out = BatchedFitter(js, slots=slots, device=dev).run()
+        out = BatchedFitter(js, slots=slots, device=dev, pixel_budget=budget if slots > 1 else None).run()
         e1.record()
         torch.cuda.synchronize()
         sec = e0.elapsed_time(e1) / 1e3
         pix_it = sum(j.cfg.W * j.cfg.H * j.iters for j in js)
         res[name] = {"seconds": round(sec, 3), "fit_iterations_per_s": round(scenes * iters / sec, 1),
                      "megapixel_iterations_per_s": round(pix_it / sec / 1e6, 1), "slots": slots,
+                     "pixel_budget": budget if slots > 1 else None,
                      "fits_done": len(out), "overflowed": sum(int(r.overflowed) for r in out)}
         del out, js
         torch.cuda.empty_cache()

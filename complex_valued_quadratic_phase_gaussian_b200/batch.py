@@ -59,9 +59,15 @@ def shard(jobs, rank, world):
 
 
 class BatchedFitter:
-    def __init__(self, jobs: List[FitJob], slots: int = 4, device="cuda", chunk: int = 64):
+    """``slots``: at most this many resident fits. ``pixel_budget`` (optional): admit a fit only
+    while the resident fits' pixels stay within the budget (one fit is always admitted), so that
+    small images run many at a time and large ones a few, with memory bounded by the budget."""
+
+    def __init__(self, jobs: List[FitJob], slots: int = 4, device="cuda", chunk: int = 64,
+                 pixel_budget: Optional[int] = None):
         self.queue = sorted(jobs, key=lambda j: -j.cost())
         self.slots = max(1, int(slots))
+        self.pixel_budget = pixel_budget
         self.device = torch.device(device)
         self.chunk = max(1, int(chunk))
         self.active = []      # [job, fitter, remaining]
@@ -70,8 +76,14 @@ class BatchedFitter:
         self._graph = None
         self._streams = [torch.cuda.Stream(self.device) for _ in range(self.slots)]
 
+    def _fits_budget(self, job):
+        if self.pixel_budget is None or not self.active:
+            return True
+        used = sum(j.cfg.W * j.cfg.H for j, _, _ in self.active)
+        return used + job.cfg.W * job.cfg.H <= self.pixel_budget
+
     def _admit(self):
-        while self.queue and len(self.active) < self.slots:
+        while self.queue and len(self.active) < self.slots and self._fits_budget(self.queue[0]):
             job = self.queue.pop(0)
             cfg = job.cfg
             if cfg.num_itrs != job.iters:

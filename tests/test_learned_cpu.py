@@ -61,3 +61,19 @@ def test_autotune_plans_factor_every_grid_of_the_configs():
         assert len(set(tuple(plan_radices(n, o)) for o in range(4))) >= 2
     hs = candidates(2816, 4480)
     assert 11 in hs and len(hs) == len(set(hs))  # 11 = the default plan with its automatic register radix
+
+
+def test_batched_fitter_pixel_budget_admission():
+    """Host logic: a job is admitted while the resident fits' pixels stay within the budget;
+    the first one always is."""
+    from types import SimpleNamespace
+    from complex_valued_quadratic_phase_gaussian_b200.batch import BatchedFitter
+    job = lambda H, W: SimpleNamespace(cfg=SimpleNamespace(H=H, W=W), iters=10, cost=lambda: H * W * 10)
+    bf = BatchedFitter.__new__(BatchedFitter)
+    bf.pixel_budget, bf.active = 1000, []
+    assert bf._fits_budget(job(100, 100))            # over the budget, but nothing is resident
+    bf.active = [[job(20, 20), None, 5]]
+    assert bf._fits_budget(job(20, 30))              # 400 + 600 = 1000
+    assert not bf._fits_budget(job(20, 31))          # 400 + 620 > 1000
+    bf.pixel_budget = None
+    assert bf._fits_budget(job(1000, 1000))

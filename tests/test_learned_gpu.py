@@ -14,7 +14,8 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def test_batched_fitter_matches_single_fits():
+@pytest.mark.parametrize("slots,budget", [(2, None), (8, 96 * 128 + 64 * 96)])
+def test_batched_fitter_matches_single_fits(slots, budget):
     from complex_valued_quadratic_phase_gaussian_b200 import learned as L
     from complex_valued_quadratic_phase_gaussian_b200.batch import BatchedFitter, FitJob
     from complex_valued_quadratic_phase_gaussian_b200.fit import Fitter
@@ -25,7 +26,7 @@ def test_batched_fitter_matches_single_fits():
         cfg = L.scene_config(H, W, it, seed=seed)
         scenes[seed] = (cfg, targets, q)
         jobs.append(FitJob(cfg, targets, q, it, init=L.grid_init(cfg, seed), tag=seed))
-    bf = BatchedFitter(jobs, slots=2, chunk=16)
+    bf = BatchedFitter(jobs, slots=slots, chunk=16, pixel_budget=budget)
     res = {r.tag: r for r in bf.run()}
     assert sorted(res) == [1, 2, 3, 4]
     for H, W, it, seed in specs:
