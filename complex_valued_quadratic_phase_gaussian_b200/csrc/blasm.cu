@@ -18,6 +18,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <initializer_list>
 #include <cstring>
 #include <vector>
 
@@ -102,16 +103,41 @@ struct RowCT {
     }
 };
 
-// The 1080p fit's rows: 2 x 2240 = 4480 = 16 x 8 x 5 x 7 (forward kernels, the
-// pruned radix 16 first) and 8 x 5 x 7 x 16 (inverse kernels, radix 16 last);
-// 320 threads = 280, 560, 896, 640 butterflies in 1, 2, 3, 2 rounds. The run-time
-// plan must be the default one (its twiddle table serves both orders).
+// Compile-time row plans (forward kernels: the pruned radix 16 first; inverse
+// kernels: radix 16 last), selected when the run-time plan is the default one
+// for that length (its twiddle table serves both orders):
+//   1080p    4480 = 16 x 8 x 5 x 7, 320 threads (280, 560, 896, 640 butterflies in 1, 2, 3, 2 rounds)
+//   512x512  1664 = 16 x 8 x 13
+//   768x1024 2688 = 16 x 8 x 3 x 7
+//   256x256  1152 = 16 x 8 x 3 x 3
 constexpr int kRow4480Threads = 320;
-using Row4480F = RowCT<kRow4480Threads, true, false, 4480, 16, 8, 5, 7>;
-using Row4480I = RowCT<kRow4480Threads, false, true, 4480, 8, 5, 7, 16>;
-static bool row_is_4480(const BlasmDev& d) {
-    const unsigned long long code = 16ull | (8ull << 5) | (5ull << 10) | (7ull << 15);
-    return d.NW == 4480 && d.row.npass == 4 && d.row.code == code;
+struct RowsRuntime {
+    using F = RowRuntime;
+    using I = RowRuntime;
+};
+struct Rows4480 {
+    using F = RowCT<kRow4480Threads, true, false, 4480, 16, 8, 5, 7>;
+    using I = RowCT<kRow4480Threads, false, true, 4480, 8, 5, 7, 16>;
+};
+struct Rows1664 {
+    using F = RowCT<kRowThreads, true, false, 1664, 16, 8, 13>;
+    using I = RowCT<kRowThreads, false, true, 1664, 8, 13, 16>;
+};
+struct Rows2688 {
+    using F = RowCT<kRowThreads, true, false, 2688, 16, 8, 3, 7>;
+    using I = RowCT<kRowThreads, false, true, 2688, 8, 3, 7, 16>;
+};
+struct Rows1152 {
+    using F = RowCT<kRowThreads, true, false, 1152, 16, 8, 3, 3>;
+    using I = RowCT<kRowThreads, false, true, 1152, 8, 3, 3, 16>;
+};
+
+static bool row_plan_is(const BlasmDev& d, int n, std::initializer_list<int> radices) {
+    if (d.NW != n || d.row.npass != (int)radices.size()) return false;
+    int p = 0;
+    for (int r : radices)
+        if ((int)((d.row.code >> (5 * p++)) & 31ull) != r) return false;
+    return true;
 }
 
 // K1: one padded row per CTA. The first FFT pass reads the splat field directly
@@ -562,34 +588,58 @@ static void rows_inverse_adjoint(const BlasmDev& d, const float2* A, const float
     blasm_rows_inv_adj_kernel<RF><<<d.C * in_h, RF::kThreads, rs, s>>>(d, A, in_field, grad_in);
 }
 
+template <class RP>
+static void forward_with(const BlasmDev& d, const float2* in, float2* out, float* pred, float2* A, float2* B,
+                         cudaStream_t s, StageMarks* marks) {
+    rows_forward<typename RP::F>(d, in, A, s);
+    if (marks) marks->mark(s);
+    launch_columns(false, d, A, B, s);
+    if (marks) marks->mark(s);
+    rows_inverse<typename RP::I>(d, B, out, pred, s);
+    if (marks) marks->mark(s);
+}
+
+template <class RP>
+static void backward_with(const BlasmDev& d, const float2* in_field, const float2* grad_out,
+                          const float* grad_pred, const float2* vfield, float2* grad_in, float2* A, float2* B,
+                          cudaStream_t s, StageMarks* marks) {
+    rows_forward_adjoint<typename RP::F>(d, grad_out, grad_pred, vfield, B, s);
+    if (marks) marks->mark(s);
+    launch_columns(true, d, B, A, s);
+    if (marks) marks->mark(s);
+    rows_inverse_adjoint<typename RP::I>(d, A, in_field, grad_in, s);
+    if (marks) marks->mark(s);
+}
+
+// calls f(RowsX{}) for the row plan of d
+template <typename F>
+static void with_row_plan(const BlasmDev& d, F&& f) {
+    if (row_plan_is(d, 4480, {16, 8, 5, 7}))
+        f(Rows4480{});
+    else if (row_plan_is(d, 1664, {16, 8, 13}))
+        f(Rows1664{});
+    else if (row_plan_is(d, 2688, {16, 8, 3, 7}))
+        f(Rows2688{});
+    else if (row_plan_is(d, 1152, {16, 8, 3, 3}))
+        f(Rows1152{});
+    else
+        f(RowsRuntime{});
+}
+
 void blasm_forward(const BlasmDev& d, const float2* in, float2* out, float* pred, void* workspace, cudaStream_t s,
                    StageMarks* marks) {
     float2 *A, *B;
     carve(d, workspace, &A, &B);
-    const bool ct = row_is_4480(d);
-    if (ct) rows_forward<Row4480F>(d, in, A, s); else rows_forward<RowRuntime>(d, in, A, s);
-    if (marks) marks->mark(s);
-    launch_columns(false, d, A, B, s);
-    if (marks) marks->mark(s);
-    if (ct) rows_inverse<Row4480I>(d, B, out, pred, s); else rows_inverse<RowRuntime>(d, B, out, pred, s);
-    if (marks) marks->mark(s);
+    with_row_plan(d, [&](auto rp) { forward_with<decltype(rp)>(d, in, out, pred, A, B, s, marks); });
 }
 
 void blasm_backward(const BlasmDev& d, const float2* in_field, const float2* grad_out, const float* grad_pred,
                     const float2* vfield, float2* grad_in, void* workspace, cudaStream_t s, StageMarks* marks) {
     float2 *A, *B;
     carve(d, workspace, &A, &B);
-    const bool ct = row_is_4480(d);
-    if (ct)
-        rows_forward_adjoint<Row4480F>(d, grad_out, grad_pred, vfield, B, s);
-    else
-        rows_forward_adjoint<RowRuntime>(d, grad_out, grad_pred, vfield, B, s);
-    if (marks) marks->mark(s);
-    launch_columns(true, d, B, A, s);
-    if (marks) marks->mark(s);
-    if (ct) rows_inverse_adjoint<Row4480I>(d, A, in_field, grad_in, s);
-    else rows_inverse_adjoint<RowRuntime>(d, A, in_field, grad_in, s);
-    if (marks) marks->mark(s);
+    with_row_plan(d, [&](auto rp) {
+        backward_with<decltype(rp)>(d, in_field, grad_out, grad_pred, vfield, grad_in, A, B, s, marks);
+    });
 }
 
 static bool fits(const BlasmDev& d) {

@@ -2,6 +2,8 @@
 // shared by blasm.cu and the per-radix instantiation units blasm_cols_r*.cu.
 #pragma once
 
+#include <initializer_list>
+
 #include "blasm.cuh"
 
 namespace cvqpg {
@@ -96,8 +98,8 @@ struct ColSplit {
 // ---------------------------------------------------------------------------
 // Head passes of the column FFT: every pass of the plan except the radix held
 // in registers. HeadRuntime follows the plan read at run time (any supported
-// length); HeadCT2<N, RA, RB> is a two-pass head fixed at compile time
-// (N = RA * RB * RL), so its strides, index splits and padded shared-memory
+// length); HeadCT<N, R...> is a head fixed at compile time
+// (N = R... * RL), so its strides, index splits and padded shared-memory
 // addresses fold into constants and no per-pass radix dispatch is compiled in.
 // ---------------------------------------------------------------------------
 struct HeadRuntime {
@@ -119,26 +121,40 @@ struct HeadRuntime {
 
 // The BLASM columns are zero-padded 2x: a forward column FFT's input is zero
 // outside rows [N/4, 3N/4), and only rows inside [N/4, 3N/4) of an inverse one
-// are kept (the output crop is at most the padded height). So the first forward
-// pass loads 8 of its 16 inputs and the last inverse pass forms 8 of its 16
-// outputs (ct_pass MID_IN / MID_OUT).
-template <int N, int RA, int RB>
-struct HeadCT2 {
+// are kept (the output crop is at most the padded height). So a radix-16 first
+// forward pass loads 8 of its 16 inputs and a radix-16 last inverse pass forms
+// 8 of its 16 outputs (ct_pass MID_IN / MID_OUT).
+template <int... R>
+struct PassList;
+template <int R0, int... Rest>
+struct PassList<R0, Rest...> {
+    static constexpr int first = R0;
+    static constexpr int last = sizeof...(Rest) == 0 ? R0 : PassList<Rest...>::last;
+    static constexpr int prod = R0 * PassList<Rest...>::prod;
+};
+template <>
+struct PassList<> {
+    static constexpr int first = 0, last = 0, prod = 1;
+};
+
+template <int N, int... R>
+struct HeadCT {
     static constexpr int kN = N;
-    static_assert(RA == 16 && RB == 16, "the middle-half passes are radix 16");
+    static constexpr int kPasses = (int)sizeof...(R);
+    static constexpr int kRL = N / PassList<R...>::prod;
     template <typename Src>
     __device__ static __forceinline__ float2* forward(Src src, float2* b0, float2* b1, int, int, const ColSplit&,
                                                       const float2* tw) {
-        ct_pass<kColThreads, N, RA, 1, false, true, false>(ElemLoadF<Src>{src}, SmemStoreF<kColPad>{b0}, tw);
-        ct_pass<kColThreads, N, RB, RA, false>(SmemLoadF<kColPad>{b0}, SmemStoreF<kColPad>{b1}, tw);
-        return b1;
+        float2* res = (kPasses % 2 == 1) ? b0 : b1;  // the buffer the last pass does not read
+        CtFft<kColPad, kColThreads, N, false, 1, PassList<R...>::first == 16, false, R...>::run(
+            ElemLoadF<Src>{src}, SmemStoreF<kColPad>{res}, b0, b1, tw);
+        return res;
     }
     template <typename Sink>
     __device__ static __forceinline__ void inverse(Sink sink, float2* b0, float2* b1, int, int, int,
                                                    const ColSplit&, const float2* tw) {
-        constexpr int RL = N / (RA * RB);
-        ct_pass<kColThreads, N, RA, RL, true>(SmemLoadF<kColPad>{b0}, SmemStoreF<kColPad>{b1}, tw);
-        ct_pass<kColThreads, N, RB, RL * RA, true, false, true>(SmemLoadF<kColPad>{b1}, ElemStoreF<Sink>{sink}, tw);
+        CtFft<kColPad, kColThreads, N, true, kRL, false, PassList<R...>::last == 16, R...>::run(
+            SmemLoadF<kColPad>{b0}, ElemStoreF<Sink>{sink}, b1, b0, tw);
     }
 };
 
@@ -358,10 +374,26 @@ void launch_cols_reg_t(bool adjoint, const BlasmDev& d, const ColSplit& cs, cons
     }
 }
 
-// Column kernels with a compile-time head for the grids the fit uses most; false
-// when (d, cs) is not one of them (the run-time plan variants apply).
+// Column kernels with a compile-time head for the grids the fits use most; false
+// when (d, cs) is not one of them (the run-time plan variants apply). One
+// translation unit per grid (blasm_cols_ct*.cu).
 bool launch_cols_ct(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
                     cudaStream_t s);
+bool launch_cols_ct_1664(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                         cudaStream_t s);
+bool launch_cols_ct_2176(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                         cudaStream_t s);
+bool launch_cols_ct_1152(bool adjoint, const BlasmDev& d, const ColSplit& cs, const float2* in, float2* out,
+                         cudaStream_t s);
+
+// the split (register radix, butterflies per thread, head radices in order) of a column plan
+inline bool col_split_is(const ColSplit& cs, int rl, int mb, std::initializer_list<int> head) {
+    if (cs.rl != rl || cs.mb != mb || cs.head_npass != (int)head.size()) return false;
+    int p = 0;
+    for (int r : head)
+        if ((int)((cs.head_code >> (5 * p++)) & 31ull) != r) return false;
+    return true;
+}
 
 // Instantiate the forward and adjoint register-spectrum kernels for one radix.
 #define CVQPG_DEFINE_COLS_REG(RL)                                                                                  \

@@ -132,3 +132,26 @@ def test_rgb_1080p_compile_time_plans_match_run_time_plans():
     ga, gb, gc = (p.backward(f, g).cpu().numpy() for p in (a, b, c))
     assert rel_l2(va, vb) < 1e-5 and rel_l2(va, vc) < 1e-5
     assert rel_l2(ga, gb) < 1e-5 and rel_l2(ga, gc) < 1e-5
+
+
+@pytest.mark.parametrize("H,W,col_hint", [(512, 512, 16), (768, 1024, 8), (256, 256, 16)])
+def test_compile_time_plans_of_the_other_grids_match_run_time_plans(H, W, col_hint):
+    """The compile-time FFT plans of the 512x512 (1664^2), 768x1024 (2176 x 2688) and 256x256
+    (1152^2) grids against the run-time plans of the same grids: `col_hint` moves the column split
+    off the compiled one, plan_hint 2 << 8 the row radix order. Within 1e-5 relative L2."""
+    from complex_valued_quadratic_phase_gaussian_b200.propagator import (BlasmPlan, reference_distances,
+                                                                         reference_pad_size)
+    rng = np.random.default_rng(H + W)
+    pad = reference_pad_size((W, H))
+    wl = [639e-9, 515e-9, 473e-9]
+    dist = reference_distances(3, 1e-3, 1e-3)
+    plans = [BlasmPlan(3, H, W, pad, wl, dist, 3.74e-6, aperture_radius=10 * max(H, W), plan_hint=h)
+             for h in (0, col_hint, 2 << 8)]
+    f = torch.from_numpy(_random_field(rng, 3, H, W)).cuda()
+    g = torch.from_numpy((rng.normal(size=(3, 3, H, W)) + 1j * rng.normal(size=(3, 3, H, W))).astype(np.complex64))
+    g = g.cuda()
+    v = [p.forward(f).cpu().numpy() for p in plans]
+    a = [p.backward(f, g).cpu().numpy() for p in plans]
+    for i in (1, 2):
+        assert rel_l2(v[0], v[i]) < 1e-5, (i, rel_l2(v[0], v[i]))
+        assert rel_l2(a[0], a[i]) < 1e-5, (i, rel_l2(a[0], a[i]))
