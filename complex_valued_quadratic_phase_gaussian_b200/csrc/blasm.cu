@@ -98,7 +98,7 @@ struct RowCT {
     template <bool INV, typename Src>
     __device__ static __forceinline__ float2* run(Src src, float2* b0, float2* b1, int, const BlasmDev& d) {
         float2* res = (kPasses % 2 == 1) ? b0 : b1;  // the buffer the last pass does not read
-        CtFft<5, NT, N, INV, 1, MI, MO, R...>::run(ElemLoadF<Src>{src}, SmemStoreF<5>{res}, b0, b1, d.row.tw);
+        CtFft<5, NT, N, INV, 1, MI, MO, true, R...>::run(ElemLoadF<Src>{src}, SmemStoreF<5>{res}, b0, b1, d.row.tw);
         return res;
     }
 };

@@ -104,6 +104,7 @@ struct ColSplit {
 // ---------------------------------------------------------------------------
 struct HeadRuntime {
     static constexpr int kN = 0;
+    static constexpr bool kEvenPasses = false;  // not known at compile time: every barrier is kept
     // forward head from stride 1 (first pass reads through src); returns the result buffer
     template <typename Src>
     __device__ static __forceinline__ float2* forward(Src src, float2* b0, float2* b1, int ld, int n,
@@ -141,19 +142,23 @@ template <int N, int... R>
 struct HeadCT {
     static constexpr int kN = N;
     static constexpr int kPasses = (int)sizeof...(R);
+    static constexpr bool kEvenPasses = kPasses % 2 == 0;
     static constexpr int kRL = N / PassList<R...>::prod;
     template <typename Src>
     __device__ static __forceinline__ float2* forward(Src src, float2* b0, float2* b1, int, int, const ColSplit&,
                                                       const float2* tw) {
         float2* res = (kPasses % 2 == 1) ? b0 : b1;  // the buffer the last pass does not read
-        CtFft<kColPad, kColThreads, N, false, 1, PassList<R...>::first == 16, false, R...>::run(
+        CtFft<kColPad, kColThreads, N, false, 1, PassList<R...>::first == 16, false, true, R...>::run(
             ElemLoadF<Src>{src}, SmemStoreF<kColPad>{res}, b0, b1, tw);
         return res;
     }
     template <typename Sink>
     __device__ static __forceinline__ void inverse(Sink sink, float2* b0, float2* b1, int, int, int,
                                                    const ColSplit&, const float2* tw) {
-        CtFft<kColPad, kColThreads, N, true, kRL, false, PassList<R...>::last == 16, R...>::run(
+        // With an even number of passes the last one reads b1, and the caller's next write
+        // of b1 (the second pass of the next plane) comes after that plane's first barrier:
+        // the closing barrier is left out.
+        CtFft<kColPad, kColThreads, N, true, kRL, false, PassList<R...>::last == 16, !kEvenPasses, R...>::run(
             SmemLoadF<kColPad>{b0}, ElemStoreF<Sink>{sink}, b1, b0, tw);
     }
 };
@@ -318,7 +323,10 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_adj_reg_kernel(Blas
                 }
             }
         }
-        __syncthreads();
+        // The pass above read `buf`. With an even number of head passes that is b1, which the
+        // next plane first writes in its second pass, after its first pass's barrier; and the
+        // final inverse below first writes b0. Otherwise buf is b0 and this barrier is needed.
+        if (!Head::kEvenPasses) __syncthreads();
     }
 #pragma unroll
     for (int b = 0; b < MB; b++) {

@@ -379,8 +379,10 @@ struct ElemStoreF {  // element writes through sink(0, a, v)
 // [N/4, 3N/4), i.e. outside r in [R/4, 3R/4); only those elements are loaded.
 // MID_OUT (last pass, NS = N/R): only the middle half of the output is used;
 // only r in [R/4, 3R/4) is formed and stored. Both for R = 16.
-template <int NT, int N, int R, int NS, bool INV, bool MID_IN = false, bool MID_OUT = false, typename Load,
-          typename Store>
+// SYNC = false leaves out the closing barrier, for a caller that has shown the
+// next writes of the buffers this pass reads come after another barrier.
+template <int NT, int N, int R, int NS, bool INV, bool MID_IN = false, bool MID_OUT = false, bool SYNC = true,
+          typename Load, typename Store>
 __device__ __forceinline__ void ct_pass(const Load& load, const Store& store, const float2* tw) {
     static_assert(!(MID_IN || MID_OUT) || R == 16, "middle-half pruning is written for radix 16");
     static_assert(!MID_IN || NS == 1, "input pruning applies to the first pass");
@@ -423,24 +425,25 @@ __device__ __forceinline__ void ct_pass(const Load& load, const Store& store, co
             store.template put<NS, R>(q * NS * R + k, v);
         }
     }
-    __syncthreads();
+    if constexpr (SYNC) __syncthreads();
 }
 
 // Passes R, Rest... of length N from stride NS: the first reads through `load`,
 // the intermediate ones ping-pong a -> b -> a ..., the last writes through `last`
 // (which must not be the buffer the last pass reads: buffer (passes - 2) % 2).
-// MI / MO: middle-half pruning of the first / last pass (ct_pass MID_IN / MID_OUT).
-template <int PS, int NT, int N, bool INV, int NS, bool MI, bool MO, int R, int... Rest>
+// MI / MO: middle-half pruning of the first / last pass (ct_pass MID_IN / MID_OUT);
+// LS: the last pass ends with a barrier (ct_pass SYNC).
+template <int PS, int NT, int N, bool INV, int NS, bool MI, bool MO, bool LS, int R, int... Rest>
 struct CtFft {
     static constexpr int kPasses = 1 + (int)sizeof...(Rest);
     template <typename Load, typename Store>
     __device__ static __forceinline__ void run(const Load& load, const Store& last, float2* a, float2* b,
                                                const float2* tw) {
         if constexpr (sizeof...(Rest) == 0) {
-            ct_pass<NT, N, R, NS, INV, MI, MO>(load, last, tw);
+            ct_pass<NT, N, R, NS, INV, MI, MO, LS>(load, last, tw);
         } else {
             ct_pass<NT, N, R, NS, INV, MI, false>(load, SmemStoreF<PS>{a}, tw);
-            CtFft<PS, NT, N, INV, NS * R, false, MO, Rest...>::run(SmemLoadF<PS>{a}, last, b, a, tw);
+            CtFft<PS, NT, N, INV, NS * R, false, MO, LS, Rest...>::run(SmemLoadF<PS>{a}, last, b, a, tw);
         }
     }
 };
