@@ -225,7 +225,9 @@ __global__ void __launch_bounds__(kColThreads, 3) blasm_cols_fwd_reg_kernel(Blas
             }
         }
     }
-    __syncthreads();
+    // Each thread reads back only its own excess entries below. With an even number of head
+    // passes `buf` is b1 and the plane loop first writes b0, so no barrier is needed here.
+    if (!Head::kEvenPasses) __syncthreads();
     const int row0 = (NH >> 1) - (d.out_h >> 1), oh = d.out_h;
     for (int p = 0; p < d.P; p++) {
         const int pc = p * d.C + c;
