@@ -80,11 +80,19 @@ bool make_fft_plan(int n, FftPlan* plan, int order) {
 // ---------------------------------------------------------------------------
 // Row FFT policies: RowRuntime runs the plan read at run time; RowCT<NT, MI, MO, N, R...>
 // the plan fixed at compile time (CtFft), for the row length of the 1080p fit.
+// run_out(src, out, a0, a1, ...): the FFT of one row, then out(a, X_a) for every
+// kept output a in [a0, a1).
 struct RowRuntime {
     static constexpr int kThreads = kRowThreads;
     template <bool INV, typename Src>
     __device__ static __forceinline__ float2* run(Src src, float2* b0, float2* b1, int ld, const BlasmDev& d) {
         return fft_run(src, b0, b1, ld, 0, d.row, INV);
+    }
+    template <bool INV, typename Src, typename Out>
+    __device__ static __forceinline__ void run_out(Src src, Out out, int a0, int a1, float2* b0, float2* b1, int ld,
+                                                   const BlasmDev& d) {
+        const float2* res = fft_run(src, b0, b1, ld, 0, d.row, INV);
+        for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) out(a, res[fft_pad(a)]);
     }
 };
 
@@ -100,6 +108,17 @@ struct RowCT {
         float2* res = (kPasses % 2 == 1) ? b0 : b1;  // the buffer the last pass does not read
         CtFft<5, NT, N, INV, 1, MI, MO, true, R...>::run(ElemLoadF<Src>{src}, SmemStoreF<5>{res}, b0, b1, d.row.tw);
         return res;
+    }
+    // the last pass writes the kept outputs straight to global memory (no closing barrier:
+    // the kernel ends there)
+    template <bool INV, typename Src, typename Out>
+    __device__ static __forceinline__ void run_out(Src src, Out out, int a0, int a1, float2* b0, float2* b1, int,
+                                                   const BlasmDev& d) {
+        auto sink = [=](int, int a, float2 v) {
+            if (a >= a0 && a < a1) out(a, v);
+        };
+        CtFft<5, NT, N, INV, 1, MI, MO, false, R...>::run(ElemLoadF<Src>{src}, ElemStoreF<decltype(sink)>{sink}, b0,
+                                                          b1, d.row.tw);
     }
 };
 
@@ -152,14 +171,15 @@ __global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_fwd_kernel(BlasmDe
     const int c = blockIdx.x / d.pH, y = blockIdx.x - c * d.pH;
     const int x0 = (d.NW >> 1) - (d.pW >> 1);
     const int pW = d.pW;
-    float2* res;
+    float2* dst = A + ((size_t)c * d.pH + y) * d.NW;
+    auto out = [=](int a, float2 v) { dst[a] = v; };
     if (d.input_mode == 0) {
         const int yy = min(max(y - d.pad_h, 0), d.H - 1);
         const float wyv = __ldg(&d.wy[y]);
         const float2* src = in + ((size_t)c * d.H + yy) * d.W;
         const float* wx = d.wx;
         const int pad_w = d.pad_w, W = d.W;
-        res = RF::template run<false>(
+        RF::template run_out<false>(
             [=](int, int e) {
                 const int x = e - x0;
                 if (x < 0 || x >= pW) return make_float2(0.f, 0.f);
@@ -168,18 +188,16 @@ __global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_fwd_kernel(BlasmDe
                 const float2 u = __ldg(&src[xx]);
                 return clamp_amplitude(make_float2(u.x * w, u.y * w));
             },
-            b0, b1, ld, d);
+            out, 0, d.NW, b0, b1, ld, d);
     } else {
         const float2* src = in + ((size_t)c * d.pH + y) * d.pW;
-        res = RF::template run<false>(
+        RF::template run_out<false>(
             [=](int, int e) {
                 const int x = e - x0;
                 return (x < 0 || x >= pW) ? make_float2(0.f, 0.f) : __ldg(&src[x]);
             },
-            b0, b1, ld, d);
+            out, 0, d.NW, b0, b1, ld, d);
     }
-    float2* dst = A + ((size_t)c * d.pH + y) * d.NW;
-    for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) dst[kx] = res[fft_pad(kx)];
 }
 
 // K2 (generic variant, any plan): the spectrum stays in a third shared buffer.
@@ -222,20 +240,17 @@ __global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_inv_kernel(BlasmDe
     const int ld = fft_ld(d.NW);
     const size_t row = blockIdx.x;  // pc * out_h + y
     const float2* src = B + row * d.NW;
-    float2* res = RF::template run<true>([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, d);
     const int col0 = (d.NW >> 1) - (d.out_w >> 1);
     float2* dst = V + row * d.out_w;
-    if (pred) {
-        // also the training prediction clamp(|V|^2, 0, 1) (train_2d_gaussian_rgb.py:193-194)
-        float* pd = pred + row * d.out_w;
-        for (int x = threadIdx.x; x < d.out_w; x += blockDim.x) {
-            const float2 v = res[fft_pad(col0 + x)];
-            dst[x] = v;
-            pd[x] = fminf(v.x * v.x + v.y * v.y, 1.0f);
-        }
-    } else {
-        for (int x = threadIdx.x; x < d.out_w; x += blockDim.x) dst[x] = res[fft_pad(col0 + x)];
-    }
+    float* pd = pred ? pred + row * d.out_w : nullptr;
+    // V and the training prediction clamp(|V|^2, 0, 1) (train_2d_gaussian_rgb.py:193-194)
+    RF::template run_out<true>(
+        [=](int, int e) { return __ldg(&src[e]); },
+        [=](int a, float2 v) {
+            dst[a - col0] = v;
+            if (pd) pd[a - col0] = fminf(v.x * v.x + v.y * v.y, 1.0f);
+        },
+        col0, col0 + d.out_w, sm, sm + ld, ld, d);
 }
 
 // ---------------------------------------------------------------------------
@@ -252,12 +267,13 @@ __global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_fwd_adj_kernel(Bla
     const int row = blockIdx.x;
     const int col0 = (d.NW >> 1) - (d.out_w >> 1);
     const int ow = d.out_w;
-    float2* res;
+    float2* dst = Bt + (size_t)row * d.NW;
+    auto out = [=](int a, float2 v) { dst[a] = v; };
     if (gpred) {
         // dL/dV = 2 V dL/dpred where 0 <= |V|^2 <= 1 (clamp passes its bounds), else 0
         const float* gp = gpred + (size_t)row * ow;
         const float2* vv = Vf + (size_t)row * ow;
-        res = RF::template run<false>(
+        RF::template run_out<false>(
             [=](int, int e) {
                 const int x = e - col0;
                 if (x < 0 || x >= ow) return make_float2(0.f, 0.f);
@@ -267,18 +283,16 @@ __global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_fwd_adj_kernel(Bla
                 const float g = (v.x * v.x + v.y * v.y <= 1.0f) ? 2.0f * gpx : 0.0f;
                 return make_float2(g * v.x, g * v.y);
             },
-            sm, sm + ld, ld, d);
+            out, 0, d.NW, sm, sm + ld, ld, d);
     } else {
         const float2* src = gV + (size_t)row * ow;
-        res = RF::template run<false>(
+        RF::template run_out<false>(
             [=](int, int e) {
                 const int x = e - col0;
                 return (x < 0 || x >= ow) ? make_float2(0.f, 0.f) : __ldg(&src[x]);
             },
-            sm, sm + ld, ld, d);
+            out, 0, d.NW, sm, sm + ld, ld, d);
     }
-    float2* dst = Bt + (size_t)row * d.NW;
-    for (int kx = threadIdx.x; kx < d.NW; kx += blockDim.x) dst[kx] = res[fft_pad(kx)];
 }
 
 // K2b (generic variant): accumulator in registers over a fixed element mapping.
@@ -334,16 +348,18 @@ __global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_inv_adj_kernel(Bla
     const int ld = fft_ld(d.NW);
     const int row = blockIdx.x;  // c * in_h + y
     const float2* src = Ab + (size_t)row * d.NW;
-    float2* res = RF::template run<true>([=](int, int e) { return __ldg(&src[e]); }, sm, sm + ld, ld, d);
     const int in_w = d.input_mode == 0 ? d.W : d.pW;
     const int c0 = (d.NW >> 1) - (in_w >> 1);
     float2* dst = gin + (size_t)row * in_w;
+    auto load = [=](int, int e) { return __ldg(&src[e]); };
     if (d.input_mode == 0) {
         const float2* u = field + (size_t)row * d.W;  // the window is exactly 1 over the image
-        for (int x = threadIdx.x; x < d.W; x += blockDim.x)
-            dst[x] = clamp_amplitude_adjoint(u[x], res[fft_pad(c0 + x)]);
+        RF::template run_out<true>(
+            load, [=](int a, float2 v) { dst[a - c0] = clamp_amplitude_adjoint(u[a - c0], v); }, c0, c0 + in_w, sm,
+            sm + ld, ld, d);
     } else {
-        for (int x = threadIdx.x; x < in_w; x += blockDim.x) dst[x] = res[fft_pad(c0 + x)];
+        RF::template run_out<true>(load, [=](int a, float2 v) { dst[a - c0] = v; }, c0, c0 + in_w, sm, sm + ld, ld,
+                                   d);
     }
 }
 
