@@ -210,13 +210,21 @@ def predict(net_weights, image, depth, device="cuda"):
     return decode(Y, H, W)
 
 
+def _timed_capture(fitter):
+    """Fitter.capture() runs one iteration eagerly before recording the graph: its device time."""
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    fitter.capture()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / 1e3
+
+
 def psnr_trace(fitter, iters, eval_every):
     """Run `iters` graph-replayed iterations; returns [(fit_seconds, iteration, per-plane PSNR)]."""
     trace = [(0.0, 0, fitter.evaluate()["psnr"])]
-    spent = 0.0
-    done = 0
-    fitter.capture()  # runs one iteration
-    done += 1
+    spent = _timed_capture(fitter)  # the capture runs (and times) the first iteration
+    done = 1
     while done < iters:
         n = min(eval_every, iters - done)
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -252,13 +260,14 @@ def train_initialiser(num_scenes=64, H=256, W=256, iters=400, steps=3000, slots=
 
 
 def time_to_psnr_experiment(weights, T_ref, H=1080, W=1920, plain_iters=2000, eval_every=50, seed=0,
-                            device="cuda"):
+                            device="cuda", goal_every=10):
     """Plain (random) init vs learned init vs constant-mean init on one seeded H x W scene.
 
     The plain fit runs `plain_iters` iterations; its final per-plane PSNR is the
     goal. The other two run until every plane reaches the goal (at most
-    `plain_iters`). Times are fit-iteration time on the device (CUDA events),
-    plus, for the learned init, the prediction itself."""
+    `plain_iters`), checked every `goal_every` iterations. Times are fit-iteration
+    time on the device (CUDA events, every iteration included, evaluations
+    excluded), plus, for the learned init, the prediction itself."""
     img, depth, targets, q = make_scene(H, W, seed + 424242, device)
     out = {}
     cfg = scene_config(H, W, plain_iters, seed=seed)
@@ -277,12 +286,10 @@ def time_to_psnr_experiment(weights, T_ref, H=1080, W=1920, plain_iters=2000, ev
         cfg = scene_config(H, W, plain_iters, seed=seed)
         f = Fitter(cfg, targets, q, init={k: v.detach().cpu() for k, v in ini.items()}, device=device)
         trace = []
-        spent, done = 0.0, 0
-        f.capture()
-        done = 1
+        spent, done = _timed_capture(f), 1
         reached = None
         while done < plain_iters:
-            n = min(eval_every, plain_iters - done)
+            n = min(goal_every, plain_iters - done)
             s.record()
             f.run(n)
             e.record()
