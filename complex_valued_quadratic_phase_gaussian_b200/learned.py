@@ -274,7 +274,8 @@ def time_to_psnr_experiment(weights, T_ref, H=1080, W=1920, plain_iters=2000, ev
     plain = Fitter(cfg, targets, q, init=synthetic_init(cfg, seed), device=device)
     tr = psnr_trace(plain, plain_iters, eval_every)
     goal = tr[-1][2]
-    out["plain"] = dict(seconds=tr[-1][0], iters=plain_iters, psnr=np.round(goal, 3).tolist())
+    out["plain"] = dict(seconds=tr[-1][0], iters=plain_iters, psnr=np.round(goal, 3).tolist(),
+                        psnr_start=np.round(tr[0][2], 3).tolist())
     del plain
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record()
@@ -285,6 +286,7 @@ def time_to_psnr_experiment(weights, T_ref, H=1080, W=1920, plain_iters=2000, ev
     for name, ini, extra in (("learned", init, t_pred), ("constant", constant_init(T_ref, H, W, device), 0.0)):
         cfg = scene_config(H, W, plain_iters, seed=seed)
         f = Fitter(cfg, targets, q, init={k: v.detach().cpu() for k, v in ini.items()}, device=device)
+        p0 = f.evaluate()["psnr"]
         trace = []
         spent, done = _timed_capture(f), 1
         reached = None
@@ -303,6 +305,7 @@ def time_to_psnr_experiment(weights, T_ref, H=1080, W=1920, plain_iters=2000, ev
                 break
         out[name] = dict(seconds_to_goal=None if reached is None else reached[0],
                          iters_to_goal=None if reached is None else reached[1],
+                         psnr_start=np.round(p0, 3).tolist(),
                          psnr_at_stop=np.round(trace[-1][2], 3).tolist(),
                          fraction_of_plain=None if reached is None else reached[0] / out["plain"]["seconds"])
         if name == "learned":
