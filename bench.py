@@ -378,6 +378,7 @@ def run_ours(args, wl, dist, world, rank, local):
     e0.record(stream)
     fitter.targets.copy_(pinned_t, non_blocking=True)
     fitter.depth_plane.copy_(pinned_q, non_blocking=True)
+    fitter.refresh_targets()  # the job's targets arrived: noise range and SSIM moments
     fitter.flat.copy_(pinned_p, non_blocking=True)
     for i in range(args.steps):
         graph.replay()

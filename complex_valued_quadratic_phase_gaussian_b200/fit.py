@@ -168,14 +168,17 @@ def synthetic_init(cfg, seed=0):
 
 
 
-def compute_target_moments(p, targets):
-    """Windowed SSIM moments of fixed targets (cvqpg_loss_target_moments) for a fit's loss."""
+def compute_target_moments(p, targets, out=None):
+    """Windowed SSIM moments of fixed targets (cvqpg_loss_target_moments) for a fit's loss,
+    into `out` when given."""
     from .loss import LossParams
     lib = _lib.lib()
     P, C, H, W = p.planes, p.channels, p.height, p.width
     lp = LossParams(C, P, H, W, 1.0, 1.0, 1.0, 0.0, 0.0, 0, 0)
     nbytes = _lib.size_query(lib.cvqpg_loss_target_moments_size, ctypes.byref(lp))
-    mom = torch.empty(nbytes // 4, dtype=torch.float32, device=targets.device)
+    mom = out if out is not None else torch.empty(nbytes // 4, dtype=torch.float32, device=targets.device)
+    if mom.numel() * 4 < nbytes:
+        raise ValueError("target moments buffer too small")
     _lib.check(lib.cvqpg_loss_target_moments(ctypes.byref(lp), _lib.ptr(targets), _lib.ptr(mom), nbytes,
                                              _lib.stream_of(targets.device)), "cvqpg_loss_target_moments")
     return mom
@@ -254,19 +257,29 @@ class Fitter:
             if tuple(self.targets.shape) != (P, C, H, W) or tuple(self.depth_plane.shape) != (H, W):
                 raise ValueError("targets must be [P,C,H,W] and depth_plane [H,W]")
             self.target_range = torch.empty(P, dtype=torch.float32, device=self.device)
-            scratch = _lib.workspace(P * TARGET_RANGE_WORKSPACE_PER_PLANE, self.device)
-            _lib.check(lib.cvqpg_loss_target_range(_lib.ptr(self.targets), P, C, H, W, _lib.ptr(self.target_range),
-                                                   _lib.ptr(scratch), scratch.numel(), _lib.stream_of(self.device)),
-                       "cvqpg_loss_target_range")
+            self._range_scratch = _lib.workspace(P * TARGET_RANGE_WORKSPACE_PER_PLANE, self.device)
             self.target_moments = None
             if cfg.target_moments:
                 self.target_moments = compute_target_moments(p, self.targets)
                 p.target_moments = _lib.ptr(self.target_moments)
+            self.refresh_targets()
         if init is None:
             init = synthetic_init(cfg, cfg.seed)
         self.load_raw(init)
         self._graph = None
         self._eval_out = torch.zeros(1 + 3 * P, dtype=torch.float32, device=self.device)
+
+    def refresh_targets(self):
+        """Recompute what the loss derives from `targets` (the per-plane range of the noise and the
+        SSIM window moments) into the same buffers, so a captured graph stays valid. Call it after
+        changing `targets` in place."""
+        P, C, H, W = self.P, self.C, self.H, self.W
+        lib, dev = self._lib, self.device
+        _lib.check(lib.cvqpg_loss_target_range(_lib.ptr(self.targets), P, C, H, W, _lib.ptr(self.target_range),
+                                               _lib.ptr(self._range_scratch), self._range_scratch.numel(),
+                                               _lib.stream_of(dev)), "cvqpg_loss_target_range")
+        if self.target_moments is not None:
+            compute_target_moments(self.params, self.targets, out=self.target_moments)
 
     # -- parameters ------------------------------------------------------------------------
     def raw(self, name):

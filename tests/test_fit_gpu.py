@@ -142,3 +142,26 @@ def test_isotropic_phase_fit_reduces_loss():
     ev = f.evaluate()
     assert np.isfinite(ev["loss"]) and ev["loss"] < 0.7 * l0
     assert not f.overflowed()
+
+
+def test_refresh_targets_after_an_in_place_change():
+    """Targets changed in place plus Fitter.refresh_targets() (noise range and SSIM moments
+    recomputed into the same buffers) give the same loss and step as a fit built on the new
+    targets."""
+    from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, Fitter, synthetic_init
+    C, W, H, P, N = 3, 80, 64, 2, 160
+    ta, q = _small_scene(C, 3, W, H, P)
+    tb, _ = _small_scene(C, 9, W, H, P)
+    cfg = FitConfig(img_size=(W, H), num_gaussians=N, num_planes=P, d_val=1e-3, volume_depth=1e-3,
+                    pad_size=[96, 112], warmup_iters=1, num_itrs=6, seed=5)
+    init = synthetic_init(cfg, seed=5)
+    a = Fitter(cfg, ta, q, init=init)
+    a.targets.copy_(torch.from_numpy(tb).cuda())
+    a.refresh_targets()
+    b = Fitter(cfg, tb, q, init=init)
+    ea, eb = a.evaluate(), b.evaluate()
+    assert abs(ea["loss"] - eb["loss"]) <= 1e-6 * abs(eb["loss"])
+    np.testing.assert_allclose(ea["ssim"], eb["ssim"], rtol=1e-6)
+    a.step()
+    b.step()
+    assert abs(a.history_records(last=1)[0][1] - b.history_records(last=1)[0][1]) <= 1e-6 * abs(eb["loss"])
