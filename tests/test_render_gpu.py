@@ -72,7 +72,7 @@ def test_cuda16_lists_bit_exact_and_field(golden, name):
 
 @pytest.mark.parametrize("name", ["torch_renderer_rgb", "torch_renderer_gray"])
 def test_torch64_rule_vs_reference_torch_renderer(golden, name):
-    """North-star gate: field within 1e-4 relative L2 of the reference PyTorch renderer (same cull rule)."""
+    """Gate: field within 1e-4 relative L2 of the reference PyTorch renderer (same cull rule)."""
     from complex_valued_quadratic_phase_gaussian_b200 import rasterizer as R
     g = golden(name)
     W, H = int(g["W"]), int(g["H"])
