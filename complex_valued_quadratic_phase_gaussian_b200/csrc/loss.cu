@@ -339,55 +339,64 @@ __global__ void __launch_bounds__(kLossThreads, NM == 3 ? 4 : 3) loss_kernel(Los
     }
 }
 
-// Fixed-order block sum of one double per thread (blockDim.x == kFinalThreads).
-constexpr int kFinalThreads = 1024;
+constexpr int kFinalThreads = 1024;  // threads of the one-block finalize
 constexpr int kRangeThreads = 512;
 constexpr int kRangeBlocks = CVQPG_TARGET_RANGE_WORKSPACE_PER_PLANE / 8;  // (max, min) float pairs
 
-__device__ __forceinline__ double block_sum_fixed(double v, double* sh) {
-    sh[threadIdx.x] = v;
-    __syncthreads();
-#pragma unroll 1
-    for (int s = kFinalThreads / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-        __syncthreads();
-    }
-    const double r = sh[0];
-    __syncthreads();
-    return r;
-}
-
 // out[0] = total loss, out[1 + p] = MSE of plane p, out[1 + P + p] = SSIM of plane p,
-// out[1 + 2P + p] = loss of plane p. One block; each thread accumulates a fixed
-// strided subset of the per-tile partials in double, then a fixed-shape tree
-// adds the threads, so the result does not depend on scheduling.
+// out[1 + 2P + p] = loss of plane p. One block. Every thread accumulates a fixed
+// strided subset of the per-tile partials of all planes in double; a fixed
+// xor-shuffle tree adds each warp's lanes and warp 0 adds the 32 warp sums the
+// same way, so the result does not depend on scheduling (two barriers in all).
 __global__ void __launch_bounds__(kFinalThreads) loss_finalize_kernel(LossDev L, const float* __restrict__ partials,
                                                                       float* __restrict__ out) {
-    __shared__ double sh[kFinalThreads];
+    constexpr int kV = 3 * kMaxLossPlanes;  // (weighted L2, MSE, SSIM map sum) per plane
+    __shared__ double sh[kV][kFinalThreads / 32];
     const int per_plane = L.C * ((L.W + kLT - 1) / kLT) * ((L.H + kLT - 1) / kLT);
-    double total = 0.0;
-    for (int q = 0; q < L.P; q++) {
-        double a = 0.0, b = 0.0, c = 0.0;
-        const float* base = partials + (size_t)q * per_plane * 3;
-        for (int t = threadIdx.x; t < per_plane; t += kFinalThreads) {
-            a += base[(size_t)t * 3 + 0];
-            b += base[(size_t)t * 3 + 1];
-            c += base[(size_t)t * 3 + 2];
-        }
-        a = block_sum_fixed(a, sh);
-        b = block_sum_fixed(b, sh);
-        c = block_sum_fixed(c, sh);
-        const double mse = b * L.inv_n;
-        const double ssim = c * L.inv_nmap;
-        const double lp = a * L.inv_n + L.ssim_weight * (1.0 - ssim);
-        total += lp;
-        if (threadIdx.x == 0) {
-            out[1 + q] = (float)mse;
-            out[1 + L.P + q] = (float)ssim;
-            out[1 + 2 * L.P + q] = (float)lp;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double v[kV];
+#pragma unroll
+    for (int i = 0; i < kV; i++) v[i] = 0.0;
+#pragma unroll
+    for (int q = 0; q < kMaxLossPlanes; q++) {
+        if (q < L.P) {
+            const float* base = partials + (size_t)q * per_plane * 3;
+            for (int t = threadIdx.x; t < per_plane; t += kFinalThreads) {
+                v[3 * q + 0] += base[(size_t)t * 3 + 0];
+                v[3 * q + 1] += base[(size_t)t * 3 + 1];
+                v[3 * q + 2] += base[(size_t)t * 3 + 2];
+            }
         }
     }
-    if (threadIdx.x == 0) out[0] = (float)total;
+#pragma unroll
+    for (int i = 0; i < kV; i++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+        if (lane == 0) sh[i][w] = v[i];
+    }
+    __syncthreads();
+    if (w == 0) {
+        double total = 0.0;
+        for (int q = 0; q < L.P; q++) {
+            double r[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                r[k] = sh[3 * q + k][lane];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) r[k] += __shfl_xor_sync(0xffffffffu, r[k], o);
+            }
+            const double mse = r[1] * L.inv_n;
+            const double ssim = r[2] * L.inv_nmap;
+            const double lp = r[0] * L.inv_n + L.ssim_weight * (1.0 - ssim);
+            total += lp;
+            if (lane == 0) {
+                out[1 + q] = (float)mse;
+                out[1 + L.P + q] = (float)ssim;
+                out[1 + 2 * L.P + q] = (float)lp;
+            }
+        }
+        if (lane == 0) out[0] = (float)total;
+    }
 }
 
 // Per-plane noise scale max(T_p) - min(T_p) (the ratio is applied later).
