@@ -63,16 +63,16 @@ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2
 // phi + k*base is unbounded, so reducing first keeps the error at ~1e-7 rad for
 // any |x| below ~1e6 instead of growing with |x|.
 // ---------------------------------------------------------------------------
-// n = nearest integer to x/(2 pi) by adding and subtracting 1.5 * 2^23 (the
-// float addition rounds to nearest, ties to even, exactly like rintf for
-// |x/(2 pi)| < 2^22): two additions on the FMA pipe instead of a rounding
-// conversion.
+// n = an integer nearest to x/(2 pi): x/(2 pi) + 1.5 * 2^23 in one FMA (rounded
+// to an integer there, for |x/(2 pi)| < 2^22), minus 1.5 * 2^23. A half-way
+// case may round the other way than rintf(x * (1/2 pi)) would; then r moves by
+// one turn to just outside [-pi, pi], which leaves sin and cos unchanged.
 __device__ __forceinline__ void sincos_reduced(float x, float* s, float* c) {
     const float kInv2Pi = 0.15915494309189535f;
     const float k2PiHi = 6.28318548202514648f;       // float(2*pi)
     const float k2PiLo = -1.7484555314695172e-07f;   // 2*pi - float(2*pi)
     const float kRound = 12582912.0f;                 // 1.5 * 2^23
-    const float n = __fsub_rn(__fadd_rn(__fmul_rn(x, kInv2Pi), kRound), kRound);
+    const float n = __fsub_rn(__fmaf_rn(x, kInv2Pi, kRound), kRound);
     float r = fmaf(-n, k2PiHi, x);
     r = fmaf(-n, k2PiLo, r);
     __sincosf(r, s, c);

@@ -494,8 +494,17 @@ __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
         __syncthreads();
         if (b + t < range.y) {
             const int g = point_list[b + t];
+            float4 v[NV];
 #pragma unroll
-            for (int q = 0; q < NV; q++) s_rec[t][q] = __ldg(&rec[(size_t)g * 4 + q]);
+            for (int q = 0; q < NV; q++) v[q] = __ldg(&rec[(size_t)g * 4 + q]);
+            const float op = v[1].y;  // colours staged pre-multiplied by the opacity
+            v[2].x *= op;
+            if (C > 1) {
+                v[2].y *= op;
+                v[2].z *= op;
+            }
+#pragma unroll
+            for (int q = 0; q < NV; q++) s_rec[t][q] = v[q];
         }
         __syncthreads();
         const int cnt = min(kTilePixels, range.y - b);
@@ -506,7 +515,7 @@ __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
             const float mahal = dx * (r0.z * dx + r0.w * dy) + dy * (r0.w * dx + r1.x * dy);
             if (!__any_sync(0xffffffffu, mahal < kMahalCut)) continue;
             const float power = fmaxf(-0.5f * mahal, -50.0f);
-            const float alpha = r1.y * __expf(power);
+            const float G = __expf(power);
             // Mahalanobis QPF (c m area) or, with ISO, the isotropic form (c |r - mu|^2)
             const float base = ISO ? 0.5f * r1.z * (dx * dx + dy * dy) * dxy2 : 0.5f * r1.z * mahal * r1.w * dxy2;
             const float4 r2 = s_rec[j][2];
@@ -527,7 +536,7 @@ __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
             for (int c = 0; c < C; c++) {
                 float s, co;
                 sincos_reduced(ph[c] + kc[c] * base, &s, &co);
-                const float amp = col[c] * alpha;
+                const float amp = col[c] * G;  // colour x opacity (folded at staging) x G
                 acc_r[c] = fmaf(amp, co, acc_r[c]);
                 acc_i[c] = fmaf(amp, s, acc_i[c]);
             }
