@@ -200,6 +200,19 @@ def kernels_per_fit_step(cfg):
     return 1 + binning + 1 + 3 + 2 + 1 + 3 + 1 + 1 + 2 + 1  # ... preprocess adjoint, Adan scalars + step, record
 
 
+DATA = "synthetic (seeded blobs + 1/f noise targets, 1/f depth; random-init Gaussians)"
+
+
+def workload_config(args, cfg, world):
+    """The `config` object of every arm's JSON line (same keys for ours and the reference)."""
+    pH, pW = cfg.resolved_pad()
+    return {"workload": f"{args.workload}_fit", "image": f"{cfg.W}x{cfg.H}", "channels": len(cfg.wavelengths),
+            "gaussians": cfg.num_gaussians, "planes": cfg.num_planes, "pad": f"{pH}x{pW}",
+            "fft_grid": f"{2 * pH}x{2 * pW}", "primitive": args.primitive, "cull": "cuda16_5sigma",
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (per-iteration working set ~GBs)"}
+
+
 def build_scene(wl, seed, device, ours=False):
     """Seeded scene and its multi-plane targets: with this library's target kernel for our arm,
     with the torch restatement of the reference's target synthesis for the reference arms."""
@@ -290,23 +303,39 @@ def cpu_sample_step(pipe, component, tiles=None):
 CPU_COMPONENTS = ("render", "propagate", "loss", "adan")
 
 
-def run_cpu_reference(wl, seed, steps, warmup):
+def run_cpu_reference(wl, seed, rounds, warmup_rounds=1):
+    """The reference CPU implementation (the oracle's torch port of the reference loop, pinned to
+    the reference loop's goldens by tests/test_oracle_fit.py) on all host threads. One round = one
+    bounded sample of each component (cpu_sample_step); the iteration time is the sum of the
+    per-component medians over `rounds` rounds after `warmup_rounds` untimed ones, extrapolated to
+    the full image / all (plane, channel) pairs / all planes."""
     threads = os.cpu_count() or 1
     pipe, cfg = make_cpu_pipeline(wl, seed, threads)
-    for i in range(warmup):
-        cpu_sample_step(pipe, CPU_COMPONENTS[i % 4])
+    for _ in range(warmup_rounds):
+        for c in CPU_COMPONENTS:
+            cpu_sample_step(pipe, c)
     samples = {c: [] for c in CPU_COMPONENTS}
-    n = max(steps, 4)
-    for i in range(n):
-        c = CPU_COMPONENTS[i % 4]
-        samples[c].append(cpu_sample_step(pipe, c))
-    per_iter = sum(statistics.mean(v) for v in samples.values())
-    sample_desc = ("round-robin component samples of one iteration: splat fwd+bwd on one row of 64-px tiles "
-                   f"(x{(cfg.H + 63) // 64}), BLASM fwd+bwd of 1 of {len(cfg.distances()) * len(cfg.wavelengths)} "
-                   f"(plane, channel) pairs (x{len(cfg.distances()) * len(cfg.wavelengths)}), loss+SSIM of 1 of "
-                   f"{cfg.num_planes} planes (x{cfg.num_planes}), full Adan step; torch {torch.__version__} CPU, "
-                   f"{threads} threads; extrapolated to one iteration")
-    return 1.0 / per_iter, threads, sample_desc, {c: statistics.mean(v) for c, v in samples.items()}
+    walls = []
+    for _ in range(max(1, rounds)):
+        t0 = time.perf_counter()
+        for c in CPU_COMPONENTS:
+            samples[c].append(cpu_sample_step(pipe, c))
+        walls.append(time.perf_counter() - t0)
+    med = {c: statistics.median(v) for c, v in samples.items()}
+    spread = {c: [round(min(v), 4), round(max(v), 4)] for c, v in samples.items()}
+    per_iter = sum(med.values())
+    pc = len(cfg.distances()) * len(cfg.wavelengths)
+    sample_desc = (f"extrapolated: per component the median of {len(walls)} bounded samples (after {warmup_rounds} "
+                   f"untimed round): splat fwd+bwd on one row of 64-px tiles (x{(cfg.H + 63) // 64}), BLASM fwd+bwd "
+                   f"of 1 of {pc} (plane, channel) pairs (x{pc}), loss+SSIM of 1 of {cfg.num_planes} planes "
+                   f"(x{cfg.num_planes}), full Adan step; torch {torch.__version__} CPU, {threads} threads")
+    return dict(value=1.0 / per_iter, cores=threads, sample=desc_trim(sample_desc), component_seconds=med,
+                component_spread=spread, seconds_per_iteration=per_iter, wall_per_round=statistics.mean(walls),
+                rounds=len(walls))
+
+
+def desc_trim(s):
+    return " ".join(s.split())
 
 
 # ----------------------------------------------------------------------------------------------
@@ -393,11 +422,16 @@ def run_ours(args, wl, dist, world, rank, local):
     d2h = rec.numel() * 4 + pinned_p.numel() * 4 / args.steps
     ev = fitter.evaluate()
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = run_reference_gpu_sample(wl, seed, dev, steps=min(args.steps, 10), warmup=2)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, desc, comp = run_cpu_reference(wl, seed, steps=4, warmup=0)
-        cpu = {"value": v, "unit": "it/s", "cores": cores, "kind": "port", "sample": desc,
-               "component_seconds": comp}
+        r = run_cpu_reference(wl, seed, rounds=3, warmup_rounds=1)
+        cpu = {"value": r["value"], "unit": "it/s", "cores": r["cores"], "kind": "port", "sample": r["sample"],
+               "component_seconds": {k: round(v, 4) for k, v in r["component_seconds"].items()},
+               "component_spread_seconds": r["component_spread"]}
 
     ttp = None
     if rank == 0 and world == 1 and args.workload == "rgb1080" and not args.no_time_to_psnr:
@@ -408,21 +442,17 @@ def run_ours(args, wl, dist, world, rank, local):
 
     if rank != 0:
         return None
-    pH, pW = cfg.resolved_pad()
     line = {
         "metric": METRIC, "value": world * args.steps / elapsed_max, "unit": "it/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded blobs + 1/f noise targets, 1/f depth; random-init Gaussians)",
-        "config": {"workload": f"{args.workload}_fit", "image": f"{cfg.W}x{cfg.H}", "channels": len(cfg.wavelengths),
-                   "gaussians": cfg.num_gaussians, "planes": cfg.num_planes, "pad": f"{pH}x{pW}",
-                   "fft_grid": f"{2 * pH}x{2 * pW}", "primitive": args.primitive, "cull": "cuda16_5sigma",
-                   "graph": True, "parallelism": f"replicas x{world}", "fft_plan_hint": fitter.plan_hint,
-                   "l2": "inputs larger than L2 (per-iteration working set ~GBs)"},
+        "data": DATA,
+        "config": workload_config(args, cfg, world),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": nbytes[dom], "ms_per_launch": stage_ms[dom]},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "graph": True, "fft_plan_hint": fitter.plan_hint,
         "e2e": {"value": world * args.steps / e2e_s, "unit": "it/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
                 "note": "public Fitter API over the same iterations as the timed run (restarted from the "
@@ -437,8 +467,16 @@ def run_ours(args, wl, dist, world, rank, local):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if ref_gpu is not None:
+        line["reference_gpu"] = ref_gpu
+        if "value" in ref_gpu:
+            line["reference_gpu"]["ours_over_reference"] = round(line["value"] / ref_gpu["value"], 2)
     if ttp is not None:
         line["time_to_psnr"] = ttp
+        plain = ttp.get("plain", {})
+        if plain.get("seconds"):
+            # the whole 2000-iteration fit (the per-iteration cost grows as the Gaussians spread)
+            line["fit_2000_it_s"] = round(plain["iters"] / plain["seconds"], 2)
     if batched is not None:
         line["batched"] = batched
     return line
@@ -515,16 +553,59 @@ def run_time_to_psnr():
 
 
 def run_reference_cpu_arm(args, wl, rank):
+    """One step = one round of bounded component samples (cpu_sample_step); ms_per_step is the wall
+    time of a round, value the extrapolated full-iteration rate."""
     if rank != 0:
         return None
-    v, cores, desc, comp = run_cpu_reference(wl, args.seed, args.steps, args.warmup)
+    from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig  # noqa: F401 (config below)
+    r = run_cpu_reference(wl, args.seed, rounds=args.steps, warmup_rounds=args.warmup)
+    v = r["value"]
+    cfg = fit_config(wl, args.seed, args.primitive)
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "it/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}_fit", "renderer": "torch tile renderer (reference)"},
-            "cpu_baseline": {"value": v, "unit": "it/s", "cores": cores, "kind": "port", "sample": desc,
-                             "component_seconds": comp},
+            "warmup": args.warmup, "ms_per_step": 1e3 * r["wall_per_round"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
+            "config": workload_config(args, cfg, 1),
+            "seconds_per_iteration_extrapolated": round(r["seconds_per_iteration"], 3),
+            "cpu_baseline": {"value": v, "unit": "it/s", "cores": r["cores"], "kind": "port", "sample": r["sample"],
+                             "component_seconds": {k: round(x, 4) for k, x in r["component_seconds"].items()},
+                             "component_spread_seconds": r["component_spread"]},
             "e2e": {"value": v, "unit": "it/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_reference_gpu_sample(wl, seed, dev, steps, warmup):
+    """The reference's GPU pipeline on the same GPU, timed outside our timed region: its own CUDA
+    rasterizer (oracle/_ref, built from the reference sources) under the torch cuFFT propagator,
+    loss + SSIM and Adan of the reference loop (oracle/torch_port.py), CUDA events around `steps`
+    iterations after `warmup`."""
+    from complex_valued_quadratic_phase_gaussian_b200.fit import synthetic_init
+    from oracle.torch_port import ReferencePipeline, load_reference_extension
+    ext = load_reference_extension()
+    if ext is None:
+        return {"unavailable": "reference CUDA extension not built (oracle/build_ref.py)"}
+    cfg = fit_config(wl, seed)
+    _, _, targets, q = build_scene(wl, seed, dev)
+    init = synthetic_init(cfg, seed)
+    torch.cuda.reset_peak_memory_stats(dev)
+    pipe = ReferencePipeline({k: v.numpy() for k, v in init.items()}, (cfg.W, cfg.H), cfg.wavelengths,
+                             cfg.pixel_pitch, cfg.resolved_pad(), cfg.distances(), cfg.resolved_aperture(), targets,
+                             q, renderer="cuda", device=dev, ext=ext)
+    for _ in range(warmup):
+        pipe.step()
+    torch.cuda.synchronize(dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        pipe.step()
+    e.record()
+    torch.cuda.synchronize(dev)
+    sec = s.elapsed_time(e) / 1e3
+    out = {"value": round(steps / sec, 3), "unit": "it/s", "steps": steps, "warmup": warmup,
+           "ms_per_step": round(1e3 * sec / steps, 3), "peak_mem_gb": round(torch.cuda.max_memory_allocated(dev) / 2 ** 30, 2),
+           "pipeline": "reference cuda/ rasterizer built for sm_100a + torch cuFFT propagator, loss+SSIM, Adan "
+                       "(reference loop order, per-iteration loss.item() and plane-0 PSNR on the host)"}
+    del pipe
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_reference_gpu_arm(args, wl, dist, world, rank, local):
@@ -557,8 +638,8 @@ def run_reference_gpu_arm(args, wl, dist, world, rank, local):
     return {"impl": "reference-gpu", "metric": METRIC, "value": world * args.steps / el, "unit": "it/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}_fit",
-                       "renderer": "reference cuda/ extension built for sm_100a + torch cuFFT propagator"},
+            "config": workload_config(args, cfg, world),
+            "renderer": "reference cuda/ extension built for sm_100a + torch cuFFT propagator",
             "peak_mem_gb": torch.cuda.max_memory_allocated(dev) / 2 ** 30}
 
 
@@ -572,6 +653,8 @@ def main():
     ap.add_argument("--primitive", default="curv", choices=["curv", "flat"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference GPU pipeline sample reported beside our line")
     ap.add_argument("--batched", type=int, default=0,
                     help="also run the batched-fitter workload with this many scenes (48 = the c3 case)")
     ap.add_argument("--batched-iters", type=int, default=500)

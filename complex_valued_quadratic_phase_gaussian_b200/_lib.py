@@ -63,6 +63,11 @@ _SIGNATURES = {
     "cvqpg_fit_step": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
     "cvqpg_fit_step_timed": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p, _i],
     "cvqpg_fit_evaluate": [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
+    "cvqpg_fit_pair_count": [_p, _p, _sz, _p, _p],
+    "cvqpg_preprocess_forward": [_p, _p, _p, _p, _p, _p, _p],
+    "cvqpg_preprocess_partials": [_i],
+    "cvqpg_preprocess_backward": [_p, _p, _p, _p, _p, _p, _p],
+    "cvqpg_wait_probe": [_i, ctypes.c_uint, _p, _p],
 }
 _RESTYPES = {"cvqpg_status_string": ctypes.c_char_p}
 

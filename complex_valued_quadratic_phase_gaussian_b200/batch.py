@@ -32,6 +32,10 @@ class FitJob:
     init: Optional[Dict[str, Any]] = None
     tag: Any = None
 
+    def __post_init__(self):
+        if int(self.iters) < 1:
+            raise ValueError(f"a fit job needs at least one iteration (got {self.iters})")
+
     def cost(self):
         return self.cfg.W * self.cfg.H * self.iters
 
@@ -90,7 +94,7 @@ class BatchedFitter:
                 cfg.num_itrs = job.iters
             f = Fitter(cfg, job.targets, job.depth_plane, init=job.init, device=self.device)
             f.step()  # first iteration eagerly: lazy per-kernel set-up stays out of the capture
-            self.active.append([job, f, job.iters - 1])
+            self.active.append([job, f, job.iters - f.iteration_count()])
         self._graph = None
 
     def _capture(self):
@@ -141,7 +145,13 @@ class BatchedFitter:
                 self._graph.replay()
             self.graph_launches += n
             for a in self.active:
-                a[2] -= n
+                job, f = a[0], a[1]
+                if f.overflowed():
+                    # the overflowed steps changed nothing: grow the fit's pair capacity and
+                    # let it run the missing iterations
+                    f.grow_pair_capacity()
+                    self._graph = None
+                a[2] = job.iters - f.iteration_count()
             if self._harvest():
                 self._graph = None  # the active set changed: capture again
                 self._admit()

@@ -171,8 +171,15 @@ __global__ void record_step_kernel(const float* __restrict__ loss_out, int nvals
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        if (status && pair_count[1]) status[0] = 1;
-        if (advance && iteration) iteration[0] = it + 1;
+        if (status) {
+            // bit 0: the tile pairs overflowed the capacity; bit 1: the loss was not finite (a
+            // NaN/Inf parameter or target; nan_to_num zeroes the gradients as the reference does)
+            const int bits = (pair_count[1] ? 1 : 0) | (nvals > 0 && !isfinite(loss_out[0]) ? 2 : 0);
+            if (bits) atomicOr(status, bits);
+        }
+        // an overflowed step applied no update (AdanDev::skip): the counter stays, so the host
+        // can enlarge the pair capacity and run the same iteration again
+        if (advance && iteration && !pair_count[1]) iteration[0] = it + 1;
     }
 }
 
@@ -313,6 +320,7 @@ static int fit_step_impl(const cvqpg_fit_params* q, float* params, float* grads,
     A.norm_partials = L.norm_partials;
     A.num_partials = preprocess_backward_blocks(N);
     A.scalars = L.adan_scalars;
+    A.skip = L.pair_count + 1;
     if (N > 0) launch_adan(A, iteration, s);
     if (marks) marks->mark(s);
     record_step_kernel<<<1, 32, 0, s>>>(L.loss_out, 0, L.pair_count, nullptr, 1, nullptr, iteration, 1);
@@ -336,6 +344,20 @@ extern "C" int cvqpg_fit_step_timed(const cvqpg_fit_params* q, float* params, fl
     m.n = num_events;
     return fit_step_impl(q, params, grads, adan_state, targets, depth_plane, target_range, iteration, history, status,
                          workspace, bytes, stream, &m);
+}
+
+extern "C" int cvqpg_fit_pair_count(const cvqpg_fit_params* q, const void* workspace, size_t bytes,
+                                    int32_t* out_device, void* stream) {
+    FitLayout L;
+    BlasmDev bd;
+    LossDev ld;
+    if (!out_device) return CVQPG_ERR_ARG;
+    const int st = fit_prepare(q, const_cast<void*>(workspace), bytes, &L, &bd, &ld);
+    if (st != CVQPG_OK) return st;
+    if (cudaMemcpyAsync(out_device, L.pair_count, 2 * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                        (cudaStream_t)stream) != cudaSuccess)
+        return CVQPG_ERR_CUDA;
+    return CVQPG_OK;
 }
 
 extern "C" int cvqpg_fit_evaluate(const cvqpg_fit_params* q, const float* params, const float* targets,

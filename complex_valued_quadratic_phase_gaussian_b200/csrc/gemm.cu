@@ -279,3 +279,21 @@ extern "C" int cvqpg_gemm_bf16_tn(const void* A, int lda, const void* B, int ldb
     return tc_gemm((const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, M, N, K, g, splits, status,
                    (cudaStream_t)stream);
 }
+
+// Self-check of the bounded wait: one thread waits on a shared-memory mbarrier
+// (count 1) with the polling loop every tcgen05 kernel here uses. With arrive = 0
+// nothing ever arrives, so the wait must give up after `limit` polls and report it.
+__global__ void wait_probe_kernel(int arrive, uint32_t limit, int* status) {
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t b = cvqpg::smem_u32(&bar);
+    cvqpg::mbar_init(b, 1);
+    cvqpg::mbar_fence_init();
+    if (arrive) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(b) : "memory");
+    status[0] = cvqpg::mbar_wait_n(b, 0, limit) ? 0 : 4;
+}
+
+extern "C" int cvqpg_wait_probe(int arrive, unsigned spin_limit, int* status, void* stream) {
+    if (!status || spin_limit == 0) return CVQPG_ERR_ARG;
+    wait_probe_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(arrive, spin_limit, status);
+    return cvqpg::launch_status();
+}

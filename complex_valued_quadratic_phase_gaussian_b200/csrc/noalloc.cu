@@ -39,7 +39,9 @@ static std::mutex g_scratch_mutex;
 static void* g_scratch_addr[64] = {nullptr};
 
 // Device address of the scratch on the current device, looked up once per
-// device (the first call on a device does this set-up).
+// device (the first call on a device does this set-up). The address is kept
+// for the life of the process, so the entry point must not be used on a device
+// after cudaDeviceReset on it (the reset ends the context the address belongs to).
 static int scratch_address(void** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CVQPG_ERR_CUDA;

@@ -45,7 +45,9 @@ __global__ void adan_scalars_kernel(AdanDev A, const int32_t* __restrict__ itera
         const double bc2 = 1.0 - pow(A.beta2, (double)step);
         const double bc3s = sqrt(1.0 - pow(A.beta3, (double)step));
         float* o = A.scalars + 8 + 8 * t;
-        o[0] = (!A.frozen_always[t] && it >= A.first_iter[t]) ? 1.0f : 0.0f;  // frozen during warm-up: no gradient
+        const bool skip = A.skip && A.skip[0] != 0;
+        // frozen during warm-up: no gradient; skipped step: nothing changes
+        o[0] = (!skip && !A.frozen_always[t] && it >= A.first_iter[t]) ? 1.0f : 0.0f;
         o[1] = (it == A.first_iter[t]) ? 1.0f : 0.0f;  // state created now: zeros, neg_pre_grad = -grad*clip
         o[2] = (float)(lr / bc1);
         o[3] = (float)(lr * A.beta2 / bc2);

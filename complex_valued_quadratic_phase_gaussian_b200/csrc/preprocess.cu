@@ -205,3 +205,64 @@ void launch_preprocess_backward(int channels, const PreDev& P, const RawParams& 
 }
 
 }  // namespace cvqpg
+
+using namespace cvqpg;
+
+static int preprocess_dev(const cvqpg_preprocess_params* q, PreDev* P) {
+    if (!q) return CVQPG_ERR_ARG;
+    if (q->channels != 1 && q->channels != 3) return CVQPG_ERR_CHANNELS;
+    if (q->num_gaussians < 0 || q->width <= 0 || q->height <= 0 || q->curv_mode < 0 || q->curv_mode > 2)
+        return CVQPG_ERR_ARG;
+    P->n = q->num_gaussians;
+    P->W = q->width;
+    P->H = q->height;
+    P->curv_mode = q->curv_mode;
+    P->curv_const = (float)q->curv_const;
+    double lam = q->wavelengths[0];
+    if (q->channels == 3)
+        for (int c = 1; c < 3; c++) lam = q->wavelengths[c] < lam ? q->wavelengths[c] : lam;
+    P->eta_lambda = (float)(q->curv_nyquist * lam);
+    P->dxy_sq = (float)(q->pixel_pitch * q->pixel_pitch);
+    P->curv_trainable = q->curv_trainable;
+    P->curv_warmup = q->curv_trainable ? q->warmup_iters : 0;
+    return CVQPG_OK;
+}
+
+static RawParams raw_views(const float* params, int N, int C) {
+    return RawParams{params, params + 2 * N, params + 4 * N, params + 5 * N, params + (5 + C) * N,
+                     params + (5 + 2 * C) * N, params + (6 + 2 * C) * N};
+}
+
+extern "C" int cvqpg_preprocess_forward(const cvqpg_preprocess_params* q, const float* params, float* records,
+                                        int32_t* radii, float* radius3, uint32_t* tiles_touched, void* stream) {
+    PreDev P;
+    const int st = preprocess_dev(q, &P);
+    if (st != CVQPG_OK) return st;
+    if (P.n > 0 && (!params || !records || !radii || !tiles_touched)) return CVQPG_ERR_ARG;
+    const int C = q->channels;
+    const BinRule rule = make_bin_rule(CVQPG_CULL_CUDA16_5SIGMA, q->width, q->height, radii, nullptr);
+    launch_preprocess_forward(C, P, raw_views(params, P.n, C), records, radii, radius3, tiles_touched, rule,
+                              (cudaStream_t)stream);
+    return launch_status();
+}
+
+extern "C" int cvqpg_preprocess_partials(int num_gaussians) { return preprocess_backward_blocks(num_gaussians); }
+
+extern "C" int cvqpg_preprocess_backward(const cvqpg_preprocess_params* q, const float* params,
+                                         const float* splat_grads, float* grads, const int32_t* iteration,
+                                         float* partials, void* stream) {
+    PreDev P;
+    const int st = preprocess_dev(q, &P);
+    if (st != CVQPG_OK) return st;
+    if (!partials || (P.n > 0 && (!params || !splat_grads || !grads))) return CVQPG_ERR_ARG;
+    const int N = P.n, C = q->channels;
+    const float* sg = splat_grads;
+    const SplatGradsIn gin{sg, sg + 2 * N, sg + 5 * N, sg + (5 + C) * N, sg + (5 + 2 * C) * N,
+                           sg + (6 + 2 * C) * N, sg + (7 + 2 * C) * N};
+    float* g = grads;
+    const RawGrads out{g, g + 2 * N, g + 4 * N, g + 5 * N, g + (5 + C) * N, g + (5 + 2 * C) * N,
+                       g + (6 + 2 * C) * N};
+    launch_preprocess_backward(C, P, raw_views(params, N, C), gin, out, iteration, partials, (cudaStream_t)stream);
+    return launch_status();
+}
+

@@ -79,6 +79,8 @@ struct AdanDev {
     const float* norm_partials;      // per-CTA sums of squares from the preprocess adjoint
     int num_partials;
     float* scalars;                  // kAdanScalars floats of scratch: the step's clip factor and step sizes
+    const int32_t* skip;             // nullable: when *skip != 0 the step leaves every tensor unchanged
+                                     // (the tile-pair list overflowed, so this step's gradient is incomplete)
 };
 
 constexpr int kAdanScalars = 8 + 8 * kParamTensors;

@@ -151,7 +151,8 @@ __global__ void scan_reduce_kernel(int n, const uint32_t* __restrict__ in, uint3
 }
 
 // Single block: exclusive scan of the block sums; writes the pair count and the
-// overflow flag. pair_count[0] is clamped to the capacity.
+// overflow flag. pair_count[0] is the true pair total (saturated at INT32_MAX);
+// the kernels that read the pairs clamp it to the capacity themselves.
 __global__ void scan_partials_kernel(int nblocks, uint32_t* __restrict__ partials, int cap,
                                      int32_t* __restrict__ pair_count) {
     // each thread handles a contiguous chunk of ceil(nblocks/blockDim) partials

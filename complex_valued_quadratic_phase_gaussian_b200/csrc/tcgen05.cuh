@@ -43,12 +43,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Wait for the phase with the given parity to complete; false after kSpinLimit polls.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i)
+// Wait for the phase with the given parity to complete; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait_n(uint32_t bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) { return mbar_wait_n(bar, parity, kSpinLimit); }
 
 // ---- TMA: one 2D tile global -> shared, completion counted on `bar` ---------
 // x is the inner (contiguous) coordinate in elements; x * element size must be a

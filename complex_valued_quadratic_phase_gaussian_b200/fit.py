@@ -75,6 +75,7 @@ class FitConfig:
     phase_iso: bool = False                  # isotropic quadratic phase (--phase_iso, model_2d_gaussian_rgb.py:356-359)
     pair_capacity: Optional[int] = None
     inject_noise: bool = True
+    max_grad_norm: float = 1.0               # clip_grad_norm_ max_norm (train_2d_gaussian_rgb.py:209); <= 0: no clip
     history_len: int = 4096
     plan_hint: int = 0                       # FFT plan of the propagation (autotune.py); 0 = defaults
     autotune: bool = False                   # pick plan_hint by measurement (cached per grid)
@@ -183,6 +184,25 @@ def compute_target_moments(p, targets, out=None):
                                              _lib.stream_of(targets.device)), "cvqpg_loss_target_moments")
     return mom
 
+def save_gaussians(raw, img_size, path):
+    """Write a checkpoint in the reference's format (Gaussians2D.save_gaussians,
+    model_2d_gaussian_rgb.py:155-167): the seven raw tensors as CPU float32 tensors and img_size,
+    under the reference's keys, so that Gaussians2D.load_gaussians and export_poh.py read it."""
+    d = {k: torch.as_tensor(raw[k], dtype=torch.float32).detach().cpu().clone() for k in RAW_KEYS}
+    d["img_size"] = tuple(int(v) for v in img_size)
+    torch.save(d, path)
+    return d
+
+
+def read_gaussians(path):
+    """Read a reference-format checkpoint: ({raw key: float32 tensor}, img_size)."""
+    d = torch.load(path, map_location="cpu")
+    missing = [k for k in RAW_KEYS if k not in d]
+    if missing:
+        raise ValueError(f"checkpoint {path} lacks {missing}")
+    return {k: d[k].detach().to(torch.float32) for k in RAW_KEYS}, tuple(int(v) for v in d.get("img_size", (0, 0)))
+
+
 class Fitter:
     """Device-resident fit of one hologram with the fused kernels."""
 
@@ -222,7 +242,7 @@ class Fitter:
             p.lr[i] = float(lr)
         for i, b in enumerate((0.98, 0.92, 0.99)):
             p.betas[i] = b
-        p.eps, p.weight_decay, p.max_grad_norm = 1e-8, 0.0, 1.0
+        p.eps, p.weight_decay, p.max_grad_norm = 1e-8, 0.0, float(cfg.max_grad_norm)
         for i in range(3):
             p.loss_weights[i] = 1.0
         p.ssim_weight = 0.025 * 0.2
@@ -236,16 +256,12 @@ class Fitter:
         self.params = p
         lib = _lib.lib()
         self._lib = lib
-        self.ws_bytes = _lib.size_query(lib.cvqpg_fit_workspace_size, ctypes.byref(p))
         total = (7 + 2 * C) * N
         self.numels = [2 * N, 2 * N, N, C * N, C * N, N, N]
         self.shapes = [(N, 2), (N, 2), (N,), (N, C), (N, C), (N,), (N,)]
+        self._lr_table = means_lr_table(cfg.lr, p.num_iters) if cfg.cosine_means else None
         with torch.cuda.device(self.device):
-            self.workspace = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
-            table = means_lr_table(cfg.lr, p.num_iters) if cfg.cosine_means else None
-            tptr = table.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if table is not None else None
-            _lib.check(lib.cvqpg_fit_setup(ctypes.byref(p), tptr, _lib.ptr(self.workspace), self.ws_bytes),
-                       "cvqpg_fit_setup")
+            self._setup_workspace()
             self.flat = torch.zeros(total, dtype=torch.float32, device=self.device)
             self.grads = torch.zeros(total, dtype=torch.float32, device=self.device)
             self.adan_state = torch.zeros(4 * total, dtype=torch.float32, device=self.device)
@@ -267,7 +283,48 @@ class Fitter:
             init = synthetic_init(cfg, cfg.seed)
         self.load_raw(init)
         self._graph = None
+        self._issued = 0        # steps issued through run()/capture (host count)
+        self._since_check = 0   # steps issued since the status was last read
         self._eval_out = torch.zeros(1 + 3 * P, dtype=torch.float32, device=self.device)
+
+    def _setup_workspace(self):
+        """(Re)carve the workspace for the current params (pair capacity included) and fill its tables."""
+        p, lib = self.params, self._lib
+        self.ws_bytes = _lib.size_query(lib.cvqpg_fit_workspace_size, ctypes.byref(p))
+        self.workspace = None
+        self.workspace = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
+        table = self._lr_table
+        tptr = table.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if table is not None else None
+        _lib.check(lib.cvqpg_fit_setup(ctypes.byref(p), tptr, _lib.ptr(self.workspace), self.ws_bytes),
+                   "cvqpg_fit_setup")
+
+    def pair_count(self):
+        """(true tile-pair total, overflowed) of the last step or evaluation (host read)."""
+        out = torch.zeros(2, dtype=torch.int32, device=self.device)
+        _lib.check(self._lib.cvqpg_fit_pair_count(ctypes.byref(self.params), _lib.ptr(self.workspace),
+                                                  self.ws_bytes, _lib.ptr(out), _lib.stream_of(self.device)),
+                   "cvqpg_fit_pair_count")
+        a = out.cpu().tolist()
+        return int(a[0]), bool(a[1])
+
+    def grow_pair_capacity(self, needed=None):
+        """Enlarge the tile-pair capacity after an overflow: to 1.25x the pair total of the last
+        step (at least double the old capacity), with a new workspace; clears the status flag and
+        drops the captured graph. The overflowed step changed nothing, so the fit resumes at the
+        same iteration."""
+        if needed is None:
+            needed, _ = self.pair_count()
+        old = int(self.params.pair_capacity)
+        new = max(2 * old, int(1.25 * needed) + 1024)
+        if new >= 2 ** 31 - 1:
+            raise RuntimeError(f"tile pairs ({needed}) exceed the int32 capacity of the binning")
+        self.params.pair_capacity = new
+        with torch.cuda.device(self.device):
+            self._setup_workspace()
+        self.status.bitwise_and_(~1)
+        self._graph = None
+        self.capacity_grown = getattr(self, "capacity_grown", 0) + 1
+        return new
 
     def refresh_targets(self):
         """Recompute what the loss derives from `targets` (the per-plane range of the noise and the
@@ -282,6 +339,12 @@ class Fitter:
             compute_target_moments(self.params, self.targets, out=self.target_moments)
 
     # -- parameters ------------------------------------------------------------------------
+    def grad(self, name):
+        """Gradient of raw parameter `name` from the last step (after nan_to_num and the clip)."""
+        i = RAW_KEYS.index(name)
+        off = sum(self.numels[:i])
+        return self.grads[off:off + self.numels[i]].view(self.shapes[i])
+
     def raw(self, name):
         i = RAW_KEYS.index(name)
         off = sum(self.numels[:i])
@@ -298,11 +361,30 @@ class Fitter:
         return d
 
     def save_gaussians(self, path):
-        torch.save(self.state_dict(), path)
+        save_gaussians({k: self.raw(k) for k in RAW_KEYS}, self.cfg.img_size, path)
+
+    def reset_optimizer(self):
+        """Fresh Adan state, iteration 0 and an empty history (the reference builds a new optimiser
+        after loading, train_2d_gaussian_rgb.py:73-86)."""
+        self.adan_state.zero_()
+        self.grads.zero_()
+        self.iteration.zero_()
+        self.history.zero_()
+        self.status.zero_()
+        self._issued = 0
+        self._since_check = 0
 
     def load_gaussians(self, path):
-        d = torch.load(path, map_location="cpu")
+        """Load a reference-format checkpoint (model_2d_gaussian_rgb.py:170-180) into this fit: the
+        image size must match; the optimiser state, iteration counter and history start afresh."""
+        d, size = read_gaussians(path)
+        if size != (self.cfg.W, self.cfg.H):
+            raise ValueError(f"checkpoint img_size {size} does not match the fit's {(self.cfg.W, self.cfg.H)}")
+        for k in RAW_KEYS:
+            if d[k].numel() != self.raw(k).numel():
+                raise ValueError(f"checkpoint {k} has {d[k].numel()} values, the fit expects {self.raw(k).numel()}")
         self.load_raw(d)
+        self.reset_optimizer()
 
     # -- iteration -------------------------------------------------------------------------
     def _step_call(self, stream):
@@ -335,9 +417,12 @@ class Fitter:
         return {name: evs[i].elapsed_time(evs[i + 1]) for i, name in enumerate(self.STAGES)}
 
     def step(self):
-        """One fit iteration (eager launches on the current stream)."""
+        """One fit iteration (eager launches on the current stream). A step whose tile pairs
+        overflow changes nothing and sets overflowed(); run() and check_status() recover from it."""
         s = torch.cuda.current_stream(self.device).cuda_stream
         _lib.check(self._step_call(s), "cvqpg_fit_step")
+        self._issued += 1
+        self._since_check += 1
 
     def capture(self):
         """Record one iteration into a CUDA graph (the iteration state is in device memory)."""
@@ -358,15 +443,48 @@ class Fitter:
         self._graph = g
         return g
 
-    def run(self, iters, graph=True):
-        if graph and self._graph is None:
-            self.capture()
-            iters -= 1
-        for _ in range(max(0, iters)):
+    def run(self, iters, graph=True, check_every=100):
+        """Advance the fit by `iters` iterations (graph replays, or eager steps). Every
+        `check_every` iterations, counted across calls, the status flag is read (one host sync):
+        if a step's tile pairs overflowed the capacity, that step changed nothing, so the capacity
+        is grown (grow_pair_capacity) and the lost iterations run again. check_status() does the
+        same check on demand (for the last iterations of a fit)."""
+        left = max(0, int(iters))
+        while left > 0:
+            n = min(left, max(1, int(check_every) - self._since_check))
+            left -= n
+            if graph and self._graph is None:
+                self.capture()  # runs (and counts) one step itself
+                n -= 1
             if graph:
-                self._graph.replay()
+                for _ in range(n):
+                    self._graph.replay()
+                self._issued += n
+                self._since_check += n
             else:
-                self.step()
+                for _ in range(n):
+                    self.step()
+            if self._since_check >= max(1, int(check_every)):
+                left += self._recover_overflow()
+
+    def check_status(self):
+        """Read the status flag now; after an overflow, grow the capacity and run the lost iterations
+        again. Returns the number of iterations that were run again."""
+        lost = self._recover_overflow()
+        if lost:
+            self.run(lost)
+            self._recover_overflow()
+        return lost
+
+    def _recover_overflow(self):
+        self._since_check = 0
+        if not self.overflowed():
+            return 0
+        done = self.iteration_count()
+        lost = max(0, self._issued - done)
+        self._issued = done
+        self.grow_pair_capacity()
+        return lost
 
     def evaluate(self, field_out=None, planes_out=None):
         """Noise-free forward at the current parameters: dict of loss, per-plane MSE/PSNR/SSIM."""
@@ -388,7 +506,12 @@ class Fitter:
         return int(self.iteration.item())
 
     def overflowed(self):
-        return bool(self.status.item())
+        """A step's tile pairs exceeded the capacity (status bit 0)."""
+        return bool(int(self.status.item()) & 1)
+
+    def nonfinite(self):
+        """A step's loss was NaN or Inf (status bit 1)."""
+        return bool(int(self.status.item()) & 2)
 
     def history_records(self, last=None):
         """(iteration, loss, mse[P], ssim[P]) for the recorded iterations (host read)."""

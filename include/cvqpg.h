@@ -103,7 +103,9 @@ CVQPG_API int cvqpg_render_forward(const float* means_2d, const float* inv_cov, 
  *   - all calls share the array: calls that can overlap on the GPU (different
  *     streams, or different host threads) race and must be serialised;
  *   - nothing in the array needs clearing between calls (every buffer is
- *     written before it is read).
+ *     written before it is read);
+ *   - the looked-up address is kept for the life of the process: do not call
+ *     this entry point on a device after cudaDeviceReset on it.
  * It calls no cudaMalloc, cudaFree or allocating library routine. */
 CVQPG_API int cvqpg_render_forward_noalloc(const float* means_2d, const float* inv_cov, const float* colours,
                                            const float* phase, const float* opacities, const float* curvature,
@@ -297,7 +299,13 @@ CVQPG_API int cvqpg_loss_forward_backward(const cvqpg_loss_params* prm, const fl
  * lr[4] rotation, lr[5] curvature.
  * history: ring of history_len records of 1 + 3P floats (cvqpg_loss_forward_backward
  * `out` layout), record (iteration % history_len) written each step.
- * status[0] is set to 1 (and stays) if a step's tile pairs exceeded pair_capacity.
+ * status[0] bit 0 is set (and stays) if a step's tile pairs exceeded pair_capacity;
+ * bit 1 if a step's loss was not finite (NaN/Inf in a parameter or target: the
+ * gradients are zeroed by nan_to_num, as in the reference, and the step goes on).
+ * A step whose pairs overflowed applies no parameter update and does not advance `iteration`: the
+ * caller enlarges pair_capacity (cvqpg_fit_pair_count gives the total needed),
+ * sets up a new workspace and runs the same iteration again. The reference never
+ * drops pairs because it sizes its sort buffers on the host every forward.
  */
 typedef struct cvqpg_fit_params {
     int channels, planes;
@@ -351,12 +359,70 @@ CVQPG_API int cvqpg_fit_step_timed(const cvqpg_fit_params* prm, float* params, f
                                    const float* targets, const uint8_t* depth_plane, const float* target_range,
                                    int32_t* iteration, float* history, int32_t* status, void* workspace,
                                    size_t workspace_bytes, void* stream, void** stage_events, int num_events);
+/* Tile pairs of the last step or evaluation that used this workspace: out_device[0] =
+ * the true pair total (saturated at INT32_MAX), out_device[1] = 1 if it exceeded
+ * pair_capacity. Two int32 copied device to device on `stream`. It replaces the
+ * reference's host read total_pairs = point_offsets[N-1].item() (cuda/raster.cu:71),
+ * which sizes its sort buffers every forward; here the host reads it only when a
+ * step reports an overflow. */
+CVQPG_API int cvqpg_fit_pair_count(const cvqpg_fit_params* prm, const void* workspace, size_t workspace_bytes,
+                                   int32_t* out_device, void* stream);
 /* Forward only (no noise, no update): out = 1 + 3P floats as in the loss; optionally
  * the splat field [C,H,W] and the plane fields V [P,C,H,W] (complex64) when non-null. */
 CVQPG_API int cvqpg_fit_evaluate(const cvqpg_fit_params* prm, const float* params, const float* targets,
                                  const uint8_t* depth_plane, const float* target_range, float* out,
                                  float* field_out, float* planes_out, int32_t* status, void* workspace,
                                  size_t workspace_bytes, void* stream);
+
+/* ---- per-Gaussian preprocessing -------------------------------------------
+ *
+ * The activations, covariance, inverse and culling radii of the fit's first
+ * stage and their adjoint, as separate calls (the fit step runs the same
+ * kernels). Reference: Gaussians2D.apply_activations (model_2d_gaussian_rgb.py:83-112;
+ * grayscale binds the curvature bound to wavelengths[0], model_2d_gaussian_grayscale.py:96),
+ * compute_2d_covariance_elements + invert_cov_2D (:114-153), the radii of
+ * Scene2D._render_cuda (:429-436) and the torch renderer's 3-sigma radius
+ * (:400-403), with the adjoint autograd would form through them plus the
+ * nan_to_num of train_2d_gaussian_rgb.py:205-208.
+ *
+ * params: the flat raw-parameter layout of cvqpg_fit_step. records [N][16]:
+ *   mx, my, inv00, inv01, inv11, opacity, curvature (activated c), area |sx sy|,
+ *   colours[C], phase mod 2 pi [C], zeros.
+ * radii [N] = ceil(5 sqrt(lambda_max)) (int32); radius3 [N] = 3 sqrt(lambda_max)
+ * (nullable); tiles_touched [N] = 16-px tiles of the CUDA renderer's rect.
+ * Backward: splat_grads = (8 + 2C) N floats, d_means [N,2] | d_inv_cov [N,3] |
+ * d_colours [N,C] | d_phase [N,C] | d_opacity [N] | d_curvature [N] | d_area [N]
+ * (the gradients of cvqpg_render_backward); grads = the raw-parameter gradients
+ * (flat layout) with nan/inf set to 0; partials [cvqpg_preprocess_partials(N)] =
+ * per-CTA sums of squares (for clip_grad_norm_). iteration (device int, nullable =
+ * 0) gates the curvature gradient during the warm-up. */
+typedef struct cvqpg_preprocess_params {
+    int channels;
+    int num_gaussians;
+    int width, height;
+    int curv_mode;          /* 0 off, 1 constant, 2 scale_aware */
+    int curv_trainable;
+    int warmup_iters;
+    double pixel_pitch;
+    double wavelengths[3];
+    double curv_nyquist;    /* 0.9 */
+    double curv_const;      /* 200 */
+} cvqpg_preprocess_params;
+
+CVQPG_API int cvqpg_preprocess_forward(const cvqpg_preprocess_params* prm, const float* params, float* records,
+                                       int32_t* radii, float* radius3, uint32_t* tiles_touched, void* stream);
+CVQPG_API int cvqpg_preprocess_partials(int num_gaussians);
+CVQPG_API int cvqpg_preprocess_backward(const cvqpg_preprocess_params* prm, const float* params,
+                                        const float* splat_grads, float* grads, const int32_t* iteration,
+                                        float* partials, void* stream);
+
+/* Self-check of the bounded mbarrier wait that every tcgen05 kernel here uses
+ * (no counterpart in the reference, which has no tensor-core code). One thread
+ * waits on a shared-memory mbarrier; with arrive = 0 nothing arrives, so the
+ * wait gives up after spin_limit polls and *status (device int) = 4; with
+ * arrive = 1 the phase completes and *status = 0. The kernel returns either way:
+ * the failure path of a timed-out pipeline wait, exercised without a fault. */
+CVQPG_API int cvqpg_wait_probe(int arrive, unsigned spin_limit, int* status, void* stream);
 
 /* ---- BF16 tensor-core GEMM (learned initialiser) ---------------------------
  *

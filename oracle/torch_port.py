@@ -105,7 +105,10 @@ class ReferencePipeline:
 
     def __init__(self, raw, img_size, wavelengths, pixel_pitch, pad, distances, aperture, targets, depth_plane,
                  renderer="torch", lrs=(0.01, 0.005, 0.0025, 0.025, 0.001, 0.001), warmup_iters=400, num_itrs=2001,
-                 device="cpu", ext=None, curv_nyquist=0.9):
+                 device="cpu", ext=None, curv_nyquist=0.9, noise=None):
+        """noise: None draws the target noise with torch.randn_like as the reference loop does
+        (utils/propagator.py:432); a callable noise(iteration) -> [P, C, H, W] standard normals
+        injects given noise instead (the parity tests use the oracle's counter-based normals)."""
         self.dev = torch.device(device)
         self.W, self.H = img_size
         self.wl = list(wavelengths)
@@ -137,6 +140,8 @@ class ReferencePipeline:
         self._sgd = torch.optim.SGD([p], lr=lrs[0])
         self._sched = torch.optim.lr_scheduler.CosineAnnealingLR(self._sgd, T_max=max(1, num_itrs), eta_min=1e-3)
         self.it = 0
+        self.noise = noise
+        self._noise_now = None
 
     # -- render ---------------------------------------------------------------------------
     def activations(self):
@@ -256,7 +261,8 @@ class ReferencePipeline:
             t = self.targets[p]
             m = self.masks[p]
             l2 = F.mse_loss(pred, t)
-            nt = t + torch.randn_like(t) * 1e-3 * (t.max() - t.min())
+            z = torch.randn_like(t) if self._noise_now is None else self._noise_now[p]
+            nt = t + z * 1e-3 * (t.max() - t.min())
             total = total + l2 + F.mse_loss(pred * m, nt * m) + F.mse_loss(pred * nt, nt * nt)
             s = ossim.ssim_torch(pred.unsqueeze(0), t.unsqueeze(0)).mean()
             total = total + 0.025 * 0.2 * (1 - s)
@@ -293,6 +299,26 @@ class ReferencePipeline:
                 p.addcdiv_(s["d"], denom, value=-g["lr"] * b2 / bc2)
                 ng.zero_().add_(grad, alpha=-1.0)
 
+    def gradients(self):
+        """The raw-parameter gradients of one iteration's loss after nan_to_num, before the clip
+        and the update (train_2d_gaussian_rgb.py:187-208); nothing is changed."""
+        trainable = set(RAW_KEYS) if self.it >= self.warmup else set(RAW_KEYS) - {"curvature"}
+        for k, p in self.params.items():
+            p.grad = None
+            p.requires_grad_(k in trainable)
+        U = soft_window_pad(self.render(), self.pad)
+        I = self.propagate(U)
+        if self.noise is not None:
+            self._noise_now = torch.as_tensor(self.noise(self.it), dtype=torch.float32, device=self.dev)
+        loss = self.loss(I, host_metrics=False)
+        self._noise_now = None
+        loss.backward()
+        out = {k: torch.nan_to_num(p.grad, nan=0.0, posinf=0.0, neginf=0.0) for k, p in self.params.items()
+               if p.grad is not None}
+        for p in self.params.values():
+            p.grad = None
+        return float(loss), out
+
     def step(self):
         trainable = set(RAW_KEYS) if self.it >= self.warmup else set(RAW_KEYS) - {"curvature"}
         for k, p in self.params.items():
@@ -300,7 +326,10 @@ class ReferencePipeline:
             p.requires_grad_(k in trainable)
         U = soft_window_pad(self.render(), self.pad)
         I = self.propagate(U)
+        if self.noise is not None:
+            self._noise_now = torch.as_tensor(self.noise(self.it), dtype=torch.float32, device=self.dev)
         loss = self.loss(I)
+        self._noise_now = None
         self.last_loss = loss.item()
         loss.backward()
         tl = [self.params[k] for k in RAW_KEYS if k in trainable]

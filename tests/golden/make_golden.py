@@ -1,8 +1,8 @@
 """Generate the golden fixtures under tests/golden/ by running the reference.
 
-This script imports the reference CVQPG Python modules from REFERENCE_DIR
-(default /root/reference, the read-only checkout present on the build machine)
-and records their outputs on small seeded inputs. The fixtures pin the CPU
+This script imports the reference CVQPG Python modules from the checkout named
+by --reference or by the environment variable CVQPG_REFERENCE_DIR (one of the
+two is required) and records their outputs on small seeded inputs. The fixtures pin the CPU
 oracle (oracle/) and the CUDA kernels to the reference's own behaviour.
 
 Reference pieces used (paths inside the reference project):
@@ -31,7 +31,7 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE_DIR = os.environ.get("CVQPG_REFERENCE_DIR", "/root/reference")
+REFERENCE_DIR = os.environ.get("CVQPG_REFERENCE_DIR")  # or --reference (main)
 sys.path.insert(0, REPO)
 
 
@@ -387,6 +387,50 @@ def golden_fit(C, name, seed, W=96, H=64, N=200, P=2, pad=(96, 128), iters=3, wa
                         **{k: v for k, v in rec.items() if k.startswith("it")})
 
 
+def golden_checkpoint(name="checkpoint", seed=71, n=50, W=40, H=24, C=3):
+    """Checkpoint format both ways: the reference's Gaussians2D.save_gaussians writes
+    checkpoint_ref.pth (model_2d_gaussian_rgb.py:155-167), and a checkpoint written by this
+    library's save_gaussians is read back by the reference's load_gaussians (:169-180); what the
+    reference loaded is recorded."""
+    import tempfile
+    from complex_valued_quadratic_phase_gaussian_b200.fit import save_gaussians
+    model = load_by_path(f"ref_model_{C}", ref("model_2d_gaussian_rgb.py"))
+    rng = np.random.default_rng(seed)
+    raw = raw_params(rng, n, W, H, C)
+    g = _make_gaussians(model, raw, W, H, C, _args_prop(C, (H + 32, W + 32)), "scale_aware")
+    g.save_gaussians(os.path.join(HERE, f"{name}_ref.pth"))
+    raw2 = raw_params(np.random.default_rng(seed + 1), n, W, H, C)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "ours.pth")
+        save_gaussians(raw2, (W, H), path)
+        g2 = model.Gaussians2D(num_points=n, img_size=(W, H), device="cpu", args_prop=_args_prop(C, (H + 32, W + 32)))
+        g2.load_gaussians(path)
+        loaded = {f"loaded_{k}": getattr(g2, k).detach().numpy().copy() for k in RAW_KEYS}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), W=W, H=H, C=C, **{f"ref_{k}": v for k, v in raw.items()},
+                        **{f"ours_{k}": v for k, v in raw2.items()}, **loaded)
+
+
+def golden_dpac(name="dpac", seed=81, C=3, W=40, H=28, pad=(64, 72)):
+    """The reference's POH encoding (export_poh.py:110-119, 175-180): soft_window_pad of a splat
+    field (model_2d_gaussian_rgb.py:186-241), phase mod 2 pi, amplitude clamped to 1, dpac(),
+    round(poh / 2 pi * 256) mod 256. export_poh.py is loaded by path; its evaluation-only imports
+    (lpips, pycvvdp: not installed) are empty stand-ins, never called here."""
+    import odak
+    for mod in ("lpips", "pycvvdp"):
+        sys.modules.setdefault(mod, types.ModuleType(mod))
+    model = load_by_path(f"ref_model_{C}", ref("model_2d_gaussian_rgb.py"))
+    exp = load_by_path("ref_export_poh", ref("export_poh.py"))
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.0, 1.4, (C, H, W))  # some amplitudes above 1: the clamp acts
+    field = (amp * np.exp(1j * rng.uniform(-np.pi, np.pi, (C, H, W)))).astype(np.complex64)
+    padded = model.soft_window_pad(torch.from_numpy(field), list(pad))
+    phase = odak.learn.wave.calculate_phase(padded) % (2 * np.pi)
+    amplitude = odak.learn.wave.calculate_amplitude(padded).clamp(0.0, 1.0)
+    levels = torch.round(exp.dpac(phase, amplitude) / (2 * np.pi) * 256).to(torch.int64) % 256
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), field=field, pad=np.array(pad),
+                        levels=levels.numpy().astype(np.uint8))
+
+
 GOLDENS = {
     "splat_rgb": lambda: golden_splat(3, "splat_rgb", 11),
     "splat_gray": lambda: golden_splat(1, "splat_gray", 12),
@@ -403,15 +447,22 @@ GOLDENS = {
     "targets_rgb": lambda: golden_targets(3, "targets_rgb", 61),
     "fit_rgb": lambda: golden_fit(3, "fit_rgb", 51),
     "fit_gray": lambda: golden_fit(1, "fit_gray", 52, P=3),
+    "checkpoint": lambda: golden_checkpoint(),
+    "dpac": lambda: golden_dpac(),
 }
 
 
 def main():
+    global REFERENCE_DIR
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*", default=None)
+    ap.add_argument("--reference", default=REFERENCE_DIR,
+                    help="the reference checkout (default: the CVQPG_REFERENCE_DIR environment variable)")
     a = ap.parse_args()
-    if not os.path.isdir(REFERENCE_DIR):
-        raise SystemExit(f"reference checkout not found at {REFERENCE_DIR}")
+    REFERENCE_DIR = a.reference
+    if not REFERENCE_DIR or not os.path.isdir(REFERENCE_DIR):
+        raise SystemExit(f"reference checkout not found ({REFERENCE_DIR!r}): pass --reference or set "
+                         "CVQPG_REFERENCE_DIR")
     torch.set_num_threads(8)
     install_third_party_restatements()
     for name, fn in GOLDENS.items():

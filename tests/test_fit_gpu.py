@@ -39,6 +39,7 @@ def test_fit_iterations_match_reference_loop(golden, name):
     f = _fitter_from_golden(g, CULL_TORCH64_3SIGMA)
     np.testing.assert_allclose(f.cfg.distances(), g["distances"])
     prev = {k: g["init_" + k].astype(np.float64) for k in RAW}
+    worst = 0.0
     for it in range(int(g["iters"])):
         f.step()
         torch.cuda.synchronize()
@@ -52,10 +53,12 @@ def test_fit_iterations_match_reference_loop(golden, name):
             assert rel_l2(got, ref) < 1e-5, (it, k, rel_l2(got, ref))
             upd_ref = ref - prev[k]
             if np.linalg.norm(upd_ref) > 0:
+                worst = max(worst, rel_l2(got - prev[k], upd_ref))
                 assert rel_l2(got - prev[k], upd_ref) < 2e-2, (it, k, rel_l2(got - prev[k], upd_ref))
             else:
                 assert np.linalg.norm(got - prev[k]) == 0, (it, k)
             prev[k] = ref
+    print(f"{name}: worst per-tensor update rel-L2 {worst:.2e}")
 
 
 def _small_scene(C, seed, W=80, H=64, P=2):
@@ -66,19 +69,26 @@ def _small_scene(C, seed, W=80, H=64, P=2):
     return targets.astype(np.float32), q
 
 
-def test_fit_step_matches_float64_oracle_cuda16_rule():
+@pytest.mark.parametrize("curv_mode", ["scale_aware", "constant", "off"])
+def test_fit_step_matches_float64_oracle_cuda16_rule(curv_mode):
+    """The curvature ablations of model_2d_gaussian_rgb.py:99-107 ('constant': 200 tanh(c),
+    'off': flat phase with the curvature tensor still in the optimiser) run through the fused
+    iteration as well as the default scale-aware bound."""
     from complex_valued_quadratic_phase_gaussian_b200.fit import (CULL_CUDA16_5SIGMA, FitConfig, Fitter,
                                                                   means_lr_table, synthetic_init)
     C, W, H, P, N = 3, 80, 64, 2, 160
     targets, q = _small_scene(C, 3, W, H, P)
     cfg = FitConfig(img_size=(W, H), num_gaussians=N, num_planes=P, d_val=1e-3, volume_depth=1e-3,
-                    pad_size=[96, 112], warmup_iters=1, num_itrs=6, cull=CULL_CUDA16_5SIGMA, seed=7)
+                    pad_size=[96, 112], warmup_iters=1, num_itrs=6, cull=CULL_CUDA16_5SIGMA, seed=7,
+                    curv_mode=curv_mode)
     init = synthetic_init(cfg, seed=7)
+    if curv_mode == "constant":  # keep c = 200 tanh(raw) in the range the scale-aware init draws from
+        init["curvature"] = init["curvature"] * 0.05
     f = Fitter(cfg, targets, q, init=init)
     orc = ofit.FitOracle({k: v.numpy() for k, v in init.items()}, W, H, cfg.wavelengths, cfg.pixel_pitch,
                          cfg.resolved_pad(), cfg.distances(), cfg.resolved_aperture(), cfg.lrs(),
                          means_lr_table=means_lr_table(cfg.lr, cfg.num_itrs), cull=osp.CULL_CUDA16_5SIGMA,
-                         warmup_iters=1, seed=7)
+                         warmup_iters=1, seed=7, curv_mode=curv_mode)
     for it in range(3):
         before = {k: f.raw(k).cpu().numpy().astype(np.float64) for k in RAW}
         f.step()
@@ -89,7 +99,9 @@ def test_fit_step_matches_float64_oracle_cuda16_rule():
             got = f.raw(k).cpu().numpy().astype(np.float64)
             assert rel_l2(got, orc.raw[k]) < 1e-5, (it, k)
             if np.linalg.norm(orc.raw[k] - before[k]) > 0:
-                assert rel_l2(got - before[k], orc.raw[k] - before[k]) < 2e-2, (it, k)
+                e = rel_l2(got - before[k], orc.raw[k] - before[k])
+                print(f"cuda16 fit ({curv_mode}) vs float64 oracle it {it} {k}: update rel-L2 {e:.2e}")
+                assert e < 2e-2, (it, k)
         # keep the two in lock-step (removes float32 drift from the comparison)
         f.load_raw({k: torch.from_numpy(orc.raw[k].astype(np.float32)) for k in RAW})
         for k in RAW:
@@ -117,16 +129,83 @@ def test_graph_replay_matches_eager_and_evaluate():
     assert not b.overflowed()
 
 
-def test_pair_capacity_overflow_is_reported():
+def test_pair_capacity_overflow_is_reported_and_recovered():
+    """A step whose tile pairs overflow the capacity applies no update and does not advance the
+    counter; Fitter.run grows the capacity and runs the iterations again, ending where a fit with
+    enough capacity from the start ends."""
     from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, Fitter, synthetic_init
     C, W, H, P, N = 1, 64, 64, 2, 200
     targets, q = _small_scene(C, 5, W, H, P)
     cfg = FitConfig(img_size=(W, H), num_gaussians=N, wavelengths=[515e-9], pixel_pitch=8e-6, num_planes=P,
                     pad_size=[96, 96], num_itrs=5, pair_capacity=64, seed=2)
-    f = Fitter(cfg, targets, q, init=synthetic_init(cfg, seed=2))
+    init = synthetic_init(cfg, seed=2)
+    f = Fitter(cfg, targets, q, init=init)
+    before = f.flat.clone()
     f.step()
     torch.cuda.synchronize()
     assert f.overflowed()
+    assert f.iteration_count() == 0 and torch.equal(f.flat, before)
+    total, over = f.pair_count()
+    assert over and total > 64
+    f.run(3, check_every=1)  # the step above overflowed: it is run again after the capacity grows
+    f.check_status()
+    assert f.iteration_count() == 4 and not f.overflowed() and f.params.pair_capacity >= total
+    cfg_ok = FitConfig(img_size=(W, H), num_gaussians=N, wavelengths=[515e-9], pixel_pitch=8e-6, num_planes=P,
+                       pad_size=[96, 96], num_itrs=5, seed=2)
+    g = Fitter(cfg_ok, targets, q, init=init)
+    g.run(4)
+    for k in RAW:
+        assert rel_l2(f.raw(k).cpu().numpy(), g.raw(k).cpu().numpy()) < 1e-6, k
+
+
+def test_nonfinite_parameter_is_detected_and_gradients_sanitised():
+    """Host-side fault injection: a NaN written into one Gaussian's colour makes the loss NaN.
+    The step reports it (status bit 1), the gradients come out of nan_to_num finite (all zero here,
+    since the NaN reaches every plane through the propagation), and the update leaves every other
+    parameter unchanged, as torch.nan_to_num + Adan do in the reference loop
+    (train_2d_gaussian_rgb.py:205-211)."""
+    from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, Fitter, synthetic_init
+    C, W, H, P, N = 3, 80, 64, 2, 160
+    targets, q = _small_scene(C, 3, W, H, P)
+    cfg = FitConfig(img_size=(W, H), num_gaussians=N, num_planes=P, d_val=1e-3, volume_depth=1e-3,
+                    pad_size=[96, 112], warmup_iters=0, num_itrs=6, seed=5)
+    f = Fitter(cfg, targets, q, init=synthetic_init(cfg, seed=5))
+    f.step()
+    assert not f.nonfinite()
+    f.raw("colours")[17, 1] = float("nan")
+    before = f.flat.clone()
+    f.step()
+    torch.cuda.synchronize()
+    assert f.nonfinite() and not f.overflowed()
+    assert not np.isfinite(f.history_records(last=1)[0][1])
+    assert torch.isfinite(f.grads).all() and float(f.grads.abs().max()) == 0.0
+    same = torch.isfinite(before)
+    assert torch.equal(f.flat[same], before[same])
+    assert f.iteration_count() == 2
+
+
+def test_evaluate_metrics_match_reference_formulas():
+    """Fitter.evaluate's per-plane PSNR is the reference's evaluation PSNR (skimage
+    peak_signal_noise_ratio with data_range 1 on the clamped, cropped intensity,
+    train_2d_gaussian_rgb.py:98-111) and its SSIM the loss's SSIM (utils/data_utils.py:22-41,
+    pytorch_msssim defaults), both recomputed in float64 from the plane fields."""
+    from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, Fitter, synthetic_init
+    from oracle import ssim as ossim
+    C, W, H, P, N = 3, 80, 64, 2, 160
+    targets, q = _small_scene(C, 3, W, H, P)
+    cfg = FitConfig(img_size=(W, H), num_gaussians=N, num_planes=P, d_val=1e-3, volume_depth=1e-3,
+                    pad_size=[96, 112], warmup_iters=1, num_itrs=20, seed=5)
+    f = Fitter(cfg, targets, q, init=synthetic_init(cfg, seed=5))
+    f.run(10)
+    V = torch.empty((P, C, H, W), dtype=torch.complex64, device="cuda")
+    ev = f.evaluate(planes_out=V)
+    pred = np.clip(np.abs(V.cpu().numpy().astype(np.complex128)) ** 2, 0.0, 1.0)
+    T = targets.astype(np.float64)
+    for p in range(P):
+        mse = np.mean((T[p] - pred[p]) ** 2)
+        assert abs(ev["psnr"][p] - 10.0 * np.log10(1.0 / mse)) < 1e-3, (p, ev["psnr"][p])
+        s_ref, _ = ossim.ssim_value_and_grad(pred[p], T[p])
+        assert abs(ev["ssim"][p] - s_ref) < 1e-5, (p, ev["ssim"][p], s_ref)
 
 
 def test_isotropic_phase_fit_reduces_loss():

@@ -95,3 +95,27 @@ def test_gemm_bias_gelu_and_dgelu_epilogues():
     g_ref[:, valid:] = 0.0
     assert rel_l2(G.float().cpu().numpy(), g_ref) < 4e-3
     assert torch.equal(Gt.cpu(), G.cpu().T.contiguous())
+
+
+def test_bounded_wait_gives_up_and_reports():
+    """The bounded mbarrier wait of the tcgen05 kernels: a barrier nothing arrives at makes it give
+    up after its poll limit with status 4 and return; with an arrival it completes with status 0.
+    The context stays usable (a GEMM runs right after)."""
+    import ctypes
+    from complex_valued_quadratic_phase_gaussian_b200 import _lib
+    lib = _lib.lib()
+    st = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    s = _lib.stream_of(torch.device("cuda"))
+    _lib.check(lib.cvqpg_wait_probe(0, 4096, _lib.ptr(st), s), "cvqpg_wait_probe")
+    torch.cuda.synchronize()
+    assert int(st.item()) == 4
+    _lib.check(lib.cvqpg_wait_probe(1, 4096, _lib.ptr(st), s), "cvqpg_wait_probe")
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    from complex_valued_quadratic_phase_gaussian_b200.mlp import gemm_bf16_tn
+    A, B = _bf16((128, 64), 1), _bf16((128, 64), 2)
+    C = torch.full((128, 128), float("nan"), device="cuda")
+    gst = gemm_bf16_tn(A.cuda(), B.cuda(), out_f32=C)
+    torch.cuda.synchronize()
+    assert int(gst.item()) == 0
+    assert rel_l2(C.cpu().numpy(), _ref(A, B)) < 1e-5

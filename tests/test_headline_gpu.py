@@ -1,0 +1,125 @@
+"""GPU: parity at the headline configuration, 1920x1080 RGB, 96,000 Gaussians, 3 planes (the
+scene and initial parameters of bench.py, seed 0).
+
+* Render (cuda/raster.cu:30-143 through the reference's own extension, oracle/_ref): per-tile
+  lists and ranges bit-exact; field within 1e-5 relative L2; all seven splat gradients within
+  1e-4 relative L2 for a random upstream gradient.
+* Fit: five fused iterations (cvqpg_fit_step) against the reference loop on the same GPU with the
+  reference CUDA renderer and the torch propagator, loss and Adan of train_2d_gaussian_rgb.py:187-211
+  (oracle/torch_port.py, pinned to the reference loop's goldens), the same targets and the same
+  injected noise. Per iteration: loss within 1e-4 relative; parameters, re-synchronised to the
+  reference's after each iteration, within 1e-5 relative L2, and the update of each tensor within
+  UPDATE_GATE relative L2 of the reference's update.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+RAW = ("means_2d", "pre_act_scales", "pre_act_rotation", "colours", "pre_act_phase", "pre_act_opacities",
+       "curvature")
+SPLAT_KEYS = ("means", "inv_cov", "colours", "phase", "opac", "curv", "area")
+W, H, N, P = 1920, 1080, 96000, 3
+WAVELENGTHS = [639e-9, 515e-9, 473e-9]
+# Adan divides each update by the running gradient magnitude, so float32 rounding differences in
+# the gradients show up in the update first.
+UPDATE_GATE = 5e-3
+
+
+@pytest.fixture(scope="module")
+def ref_ext():
+    from oracle.torch_port import load_reference_extension
+    ext = load_reference_extension()
+    if ext is None:
+        pytest.skip("reference extension not built (oracle/build_ref.py needs the reference sources)")
+    return ext
+
+
+@pytest.fixture(scope="module")
+def headline():
+    from complex_valued_quadratic_phase_gaussian_b200 import scenes
+    from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, synthetic_init
+    img, depth = scenes.rgb_blobs(H, W, seed=0)
+    targets, q = scenes.multiplane_targets_device(img, depth, P, device="cuda")
+    cfg = FitConfig(img_size=(W, H), num_gaussians=N, wavelengths=list(WAVELENGTHS), pixel_pitch=3.74e-6,
+                    num_planes=P, d_val=1e-3, volume_depth=1e-3, warmup_iters=400, num_itrs=2000, seed=0)
+    return cfg, synthetic_init(cfg, 0), targets, q
+
+
+def _pipeline(cfg, init, targets, q, ext):
+    from oracle import loss as oloss
+    from oracle.torch_port import ReferencePipeline
+    C = len(cfg.wavelengths)
+    return ReferencePipeline({k: v.numpy() for k, v in init.items()}, (cfg.W, cfg.H), cfg.wavelengths,
+                             cfg.pixel_pitch, cfg.resolved_pad(), cfg.distances(), cfg.resolved_aperture(), targets,
+                             q, renderer="cuda", warmup_iters=cfg.warmup_iters, num_itrs=cfg.num_itrs, device="cuda",
+                             ext=ext, noise=lambda it: oloss.plane_noise((P, C, cfg.H, cfg.W), cfg.seed, it))
+
+
+def test_headline_lists_field_and_gradients_vs_reference_cuda(headline, ref_ext):
+    import complex_valued_quadratic_phase_gaussian_b200 as pkg
+    cfg, init, targets, q = headline
+    pipe = _pipeline(cfg, init, targets, q, ref_ext)
+    with torch.no_grad():
+        means, scales, phase, opac, curv, cov, inv = pipe.activations()
+        c00, c01, c11 = cov
+        mid = 0.5 * (c00 + c11)
+        disc = torch.sqrt(((c00 - c11) * 0.5) ** 2 + c01 ** 2)
+        radii = (5.0 * torch.sqrt(mid + disc)).ceil().to(torch.int32)
+        ins = [t.contiguous() for t in (means, torch.stack(inv, -1), pipe.params["colours"].detach(), phase, opac,
+                                        curv, (scales[:, 0] * scales[:, 1]).abs())]
+    k = (2 * np.pi / pipe.wl_t).contiguous()
+    dxy2 = float(cfg.pixel_pitch ** 2)
+    C = 3
+    rr, ri, rpl, rranges = ref_ext.qpf_render_forward(*ins, radii, k, dxy2, W, H, C)
+    mr, mi, mpl, mranges = pkg.ext().qpf_render_forward(*ins, radii, k, dxy2, W, H, C)
+    assert rpl.numel() > 4 * N  # lists longer than one 256-entry batch exist at this size
+    assert torch.equal(rpl.cpu(), mpl.cpu()), "per-tile Gaussian lists differ"
+    assert torch.equal(rranges.cpu(), mranges.cpu()), "tile ranges differ"
+    lens = (rranges[:, 1] - rranges[:, 0]).cpu().numpy()
+    assert lens.max() > 256
+    ref_field = torch.complex(rr, ri).cpu().numpy()
+    got = torch.complex(mr, mi).cpu().numpy()
+    assert rel_l2(got, ref_field) < 1e-5
+    g = torch.Generator(device="cuda").manual_seed(3)
+    gr = torch.randn(C, H, W, device="cuda", generator=g)
+    gi = torch.randn(C, H, W, device="cuda", generator=g)
+    dref = ref_ext.qpf_render_backward(gr, gi, *ins, k, rpl, rranges, dxy2, W, H, C)
+    dgot = pkg.ext().qpf_render_backward(gr, gi, *ins, k, mpl, mranges, dxy2, W, H, C)
+    for key, a, b in zip(SPLAT_KEYS, dgot, dref):
+        e = rel_l2(a.cpu().numpy(), b.cpu().numpy())
+        print(f"headline splat gradient {key}: rel-L2 {e:.2e}")
+        assert e < 1e-4, (key, e)
+
+
+def test_headline_fit_iterations_vs_reference_loop(headline, ref_ext):
+    from complex_valued_quadratic_phase_gaussian_b200.fit import Fitter
+    cfg, init, targets, q = headline
+    pipe = _pipeline(cfg, init, targets, q, ref_ext)
+    f = Fitter(cfg, targets, q, init=init)
+    prev = {k: init[k].numpy().astype(np.float64) for k in RAW}
+    worst_upd = 0.0
+    for it in range(5):
+        f.step()
+        pipe.step()
+        torch.cuda.synchronize()
+        rec = f.history_records(last=1)[0]
+        assert rec[0] == it
+        assert abs(rec[1] - pipe.last_loss) < 1e-4 * abs(pipe.last_loss), (it, rec[1], pipe.last_loss)
+        for k in RAW:
+            got = f.raw(k).cpu().numpy().astype(np.float64)
+            ref = pipe.params[k].detach().cpu().numpy().astype(np.float64)
+            assert rel_l2(got, ref) < 1e-5, (it, k, rel_l2(got, ref))
+            upd_ref = ref - prev[k]
+            if np.linalg.norm(upd_ref) > 0:
+                e = rel_l2(got - prev[k], upd_ref)
+                worst_upd = max(worst_upd, e)
+                assert e < UPDATE_GATE, (it, k, e)
+            else:
+                assert np.linalg.norm(got - prev[k]) == 0, (it, k)
+            prev[k] = ref
+        # lock-step: start the next iteration from the reference's parameters
+        f.load_raw({k: pipe.params[k].detach() for k in RAW})
+    print(f"headline fit: worst per-tensor update rel-L2 over 5 iterations {worst_upd:.2e}")

@@ -37,3 +37,24 @@ def test_poh_levels_match_oracle_and_reconstruct():
     assert np.allclose(np.angle(ph) % (2 * np.pi), (got.astype(np.float64) * 2 * np.pi / 256) % (2 * np.pi),
                        atol=1e-5)
     assert np.all(np.isfinite(out["psnr"])) and np.all(out["psnr"] > 5.0)
+
+
+def test_poh_levels_match_reference_dpac(golden):
+    """cvqpg_poh_encode against the reference's own DPAC encoding (export_poh.py:110-119, 175-180)
+    of a seeded field: >= 99.9 % of the levels identical, the rest one level apart."""
+    import ctypes
+    from complex_valued_quadratic_phase_gaussian_b200 import _lib
+    from complex_valued_quadratic_phase_gaussian_b200.propagator import BlasmPlan
+    g = golden("dpac")
+    field = torch.from_numpy(g["field"]).cuda()
+    C, H, W = field.shape
+    pH, pW = (int(v) for v in g["pad"])
+    plan = BlasmPlan(C, H, W, (pH, pW), [639e-9, 515e-9, 473e-9][:C], [1e-3], 3.74e-6, device="cuda")
+    levels = torch.empty((C, pH, pW), dtype=torch.uint8, device="cuda")
+    _lib.check(_lib.lib().cvqpg_poh_encode(ctypes.byref(plan.params), _lib.ptr(plan.tables), plan.tables.numel(),
+                                           _lib.ptr(torch.view_as_real(field)), _lib.ptr(levels), None,
+                                           _lib.stream_of(torch.device("cuda"))), "cvqpg_poh_encode")
+    got = levels.cpu().numpy()
+    diff = (got.astype(np.int64) - g["levels"].astype(np.int64)) % 256
+    diff = np.minimum(diff, 256 - diff)
+    assert np.mean(diff == 0) >= 0.999 and diff.max() <= 1
