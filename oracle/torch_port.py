@@ -299,9 +299,10 @@ class ReferencePipeline:
                 p.addcdiv_(s["d"], denom, value=-g["lr"] * b2 / bc2)
                 ng.zero_().add_(grad, alpha=-1.0)
 
-    def gradients(self):
-        """The raw-parameter gradients of one iteration's loss after nan_to_num, before the clip
-        and the update (train_2d_gaussian_rgb.py:187-208); nothing is changed."""
+    def gradients(self, sanitize=True):
+        """The raw-parameter gradients of one iteration's loss after nan_to_num (or before it, with
+        sanitize=False), before the clip and the update (train_2d_gaussian_rgb.py:187-208);
+        nothing is changed."""
         trainable = set(RAW_KEYS) if self.it >= self.warmup else set(RAW_KEYS) - {"curvature"}
         for k, p in self.params.items():
             p.grad = None
@@ -313,11 +314,11 @@ class ReferencePipeline:
         loss = self.loss(I, host_metrics=False)
         self._noise_now = None
         loss.backward()
-        out = {k: torch.nan_to_num(p.grad, nan=0.0, posinf=0.0, neginf=0.0) for k, p in self.params.items()
-               if p.grad is not None}
+        clean = (lambda t: torch.nan_to_num(t, nan=0.0, posinf=0.0, neginf=0.0)) if sanitize else (lambda t: t.clone())
+        out = {k: clean(p.grad) for k, p in self.params.items() if p.grad is not None}
         for p in self.params.values():
             p.grad = None
-        return float(loss), out
+        return float(loss.detach()), out
 
     def step(self):
         trainable = set(RAW_KEYS) if self.it >= self.warmup else set(RAW_KEYS) - {"curvature"}
@@ -333,6 +334,12 @@ class ReferencePipeline:
         self.last_loss = loss.item()
         loss.backward()
         tl = [self.params[k] for k in RAW_KEYS if k in trainable]
+        # which Gaussians had a non-finite gradient entry this step (zeroed by nan_to_num below)
+        n = self.params["pre_act_opacities"].shape[0]
+        bad = torch.zeros(n, dtype=torch.bool, device=self.dev)
+        for p in tl:
+            bad |= ~torch.isfinite(p.grad).reshape(n, -1).all(dim=1)
+        self.last_nonfinite = bad
         for p in tl:
             p.grad = torch.nan_to_num(p.grad, nan=0.0, posinf=0.0, neginf=0.0)
         torch.nn.utils.clip_grad_norm_(tl, max_norm=1.0)

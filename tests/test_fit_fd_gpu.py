@@ -14,7 +14,14 @@ the Richardson differences <= 1e-3; the worst case and the plain h = 1e-3 figure
 The full gradient is also compared with the reference's own autograd on the same scene: the
 reference CUDA rasterizer (oracle/_ref) under the torch propagator and loss of the reference loop
 (oracle/torch_port.py, pinned to the reference loop's goldens), float32: <= 1e-3 relative L2 per
-tensor.
+tensor over the Gaussians whose reference gradient is finite. The others are a float32 quirk of
+the reference on the GPU: its amplitude clamp goes through torch.angle and torch.abs
+(train_2d_gaussian_rgb.py:91-93), and angle's backward divides by |U|^2, which underflows to 0
+where only Gaussian tails clamped at exp(-50) reach a pixel; the NaN it makes there reaches every
+Gaussian whose tile list holds that pixel, and nan_to_num (train_2d_gaussian_rgb.py:206-208) zeroes
+their whole gradient. The fused adjoint of the clamp has no such division (it is the identity for
+|U| <= 1) and matches the FP64 differences above. The test checks that the excluded Gaussians are
+exactly those with a non-finite reference gradient and that they are a minority.
 
 Memory case (3840 x 2160, 200k Gaussians, one channel, splat adjoint only):
 the render forward + adjoint fit in a few GB and the adjoint is linear in dL/dU.
@@ -96,11 +103,18 @@ def test_fused_gradient_matches_reference_autograd_512(c2_fit):
                              cfg.distances(), cfg.resolved_aperture(), c2_fit["targets"], c2_fit["q"],
                              renderer="cuda", warmup_iters=0, num_itrs=10, device="cuda", ext=ext,
                              noise=lambda it: np.zeros((P, C, H, W), np.float32))
-    loss, ref = pipe.gradients()
+    loss, raw_ref = pipe.gradients(sanitize=False)
     assert abs(loss - c2_fit["loss"]) < 1e-5 * loss
+    n = cfg.num_gaussians
+    finite = np.ones(n, bool)
     for k in RAW:
-        e = rel_l2(c2_fit["grads"][k], ref[k].cpu().numpy().astype(np.float64))
-        print(f"reference autograd {k}: rel-L2 {e:.2e}")
+        finite &= np.isfinite(raw_ref[k].cpu().numpy()).reshape(n, -1).all(axis=1)
+    print(f"reference autograd: {n - finite.sum()} of {n} Gaussians with a non-finite gradient (zeroed there)")
+    assert finite.mean() > 0.5
+    for k in RAW:
+        ref = raw_ref[k].cpu().numpy().astype(np.float64)
+        e = rel_l2(c2_fit["grads"][k][finite], ref[finite])
+        print(f"reference autograd {k}: rel-L2 {e:.2e} over the {finite.sum()} Gaussians with finite gradients")
         assert e < 1e-3, (k, e)
 
 
