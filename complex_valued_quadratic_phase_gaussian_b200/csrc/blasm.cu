@@ -248,7 +248,9 @@ __global__ void __launch_bounds__(RF::kThreads, 3) blasm_rows_inv_kernel(BlasmDe
         [=](int, int e) { return __ldg(&src[e]); },
         [=](int a, float2 v) {
             dst[a - col0] = v;
-            if (pd) pd[a - col0] = fminf(v.x * v.x + v.y * v.y, 1.0f);
+            // torch.clamp(I, 0, 1) keeps a NaN (fminf would turn it into 1)
+            const float i2 = v.x * v.x + v.y * v.y;
+            if (pd) pd[a - col0] = i2 > 1.0f ? 1.0f : i2;
         },
         col0, col0 + d.out_w, sm, sm + ld, ld, d);
 }
@@ -457,8 +459,9 @@ int blasm_make_dev(const cvqpg_blasm_params* p, const void* tables, size_t table
     d->out_h = p->out_height > 0 ? p->out_height : d->H;
     d->out_w = p->out_width > 0 ? p->out_width : d->W;
     d->input_mode = p->input_mode;
-    // one column per column-pass CTA (row-major intermediates)
-    d->G = 1;
+    // adjacent columns per column-pass CTA: four where a four-column kernel exists
+    // (blasm_cols4.cuh; row-major intermediates either way), unless the hint asks for one
+    d->G = (p->plan_hint & CVQPG_PLAN_COLS1) || (d->NW % 4) != 0 ? 1 : 4;
     if ((size_t)3 * fft_ld(d->NH) * sizeof(float2) > 227 * 1024) return CVQPG_ERR_UNSUPPORTED;
     d->scale = (float)(1.0 / ((double)d->NH * (double)d->NW));
     const int hint = p->plan_hint;

@@ -195,9 +195,13 @@ CVQPG_API int cvqpg_render_backward_cull(const float* grad_field, const float* m
  *   bits [0,5)  radix kept in registers by the column kernels (0 = automatic);
  *   bits [5,8)  radix order of the column FFTs, bits [8,11) of the row FFTs:
  *               0 radix 16 first then 8/4/2 then odd, 1 odd first then 16/8/4/2,
- *               2 radix 8 first then 4/2 then odd, 3 odd first then 8/4/2. */
+ *               2 radix 8 first then 4/2 then odd, 3 odd first then 8/4/2;
+ *   bit 11      one column per CTA in the column kernels (CVQPG_PLAN_COLS1)
+ *               instead of four adjacent columns where the grid has a four-
+ *               column kernel (column length 16 x 11 x 16 = 2816). */
 #define CVQPG_PLAN_HINT(col_radix, col_order, row_order) \
     ((col_radix) | ((col_order) << 5) | ((row_order) << 8))
+#define CVQPG_PLAN_COLS1 (1 << 11)
 
 typedef struct cvqpg_blasm_params {
     int channels;

