@@ -162,8 +162,8 @@ def test_pair_capacity_overflow_is_reported_and_recovered():
 
 
 def test_nonfinite_parameter_is_detected_and_gradients_sanitised():
-    """Host-side fault injection: a NaN written into one Gaussian's colour before the first step
-    makes the field, every plane (through the propagation) and the loss NaN, as torch.clamp
+    """Host-side fault injection: a NaN written into one Gaussian's opacity before the first step
+    makes the field of every channel, every plane (through the propagation) and the loss NaN, as torch.clamp
     propagates NaN in the reference (train_2d_gaussian_rgb.py:93, 193). The step reports it
     (status bit 1), the gradients come out of nan_to_num finite (all zero), and the first Adan
     step with a zero gradient leaves every other parameter unchanged, as torch.nan_to_num + Adan do
@@ -175,7 +175,7 @@ def test_nonfinite_parameter_is_detected_and_gradients_sanitised():
                     pad_size=[96, 112], warmup_iters=0, num_itrs=6, seed=5)
     f = Fitter(cfg, targets, q, init=synthetic_init(cfg, seed=5))
     assert not f.nonfinite()
-    f.raw("colours")[17, 1] = float("nan")
+    f.raw("pre_act_opacities")[17] = float("nan")
     before = f.flat.clone()
     f.step()
     torch.cuda.synchronize()

@@ -27,8 +27,8 @@ SPLAT_KEYS = ("means", "inv_cov", "colours", "phase", "opac", "curv", "area")
 W, H, N, P = 1920, 1080, 96000, 3
 WAVELENGTHS = [639e-9, 515e-9, 473e-9]
 # Adan divides each update by the running gradient magnitude, so float32 rounding differences in
-# the gradients show up in the update first.
-UPDATE_GATE = 2e-2
+# the gradients show up in the update first; measured on B200: <= 2.7e-5 over the five iterations.
+UPDATE_GATE = 2e-4
 
 
 @pytest.fixture(scope="module")
