@@ -7,7 +7,7 @@
 // below makes every warp access 8 rows x 4 columns: each global load or store
 // instruction of a warp moves eight whole sectors. The four transforms share
 // the CTA: shared memory holds them interleaved (element e of column g at
-// (e + e/16) * 4 + g, conflict-free for the passes' strides), and every pass
+// (e + e/16) * G + g, conflict-free for the passes' strides), and every pass
 // is one barrier for all four.
 //
 // Plan (Stockham, natural-order output, see fft.cuh): forward 16 (first pass,
@@ -19,28 +19,47 @@
 // plane; the adjoint kernel transforms each plane's gradient forward,
 // accumulates x conj(transfer) in registers and inverts once.
 //
-// Threads: 88 per column (TPC), 352 per CTA; each thread owns butterflies
-// u and u + 88 of the radix-16 passes (176 = N/16 per column) and u, u + 88,
-// u + 176 (< 256) of the radix-R2 pass (256 = N/R2 per column).
+// Threads: TPC = 176 / BPT per column; each thread owns butterflies u + b TPC
+// (b < BPT) of the radix-16 passes (176 = N/16 per column) and u + b TPC
+// (< 256) of the radix-R2 pass (256 = N/R2 per column). Measured on B200 at
+// 2816 x 4480 (forward / adjoint column stage): G = 4, BPT = 1 (704 threads,
+// 80 registers, one CTA per SM) 0.670 / 0.746 ms; G = 4, BPT = 2 (352 threads,
+// 168 registers) 0.750 / 0.797 ms; G = 2, BPT = 1 (two CTAs per SM) 0.700 /
+// 0.740 ms; the one-column kernels 0.795 / 0.753 ms. Recomputing the transfer
+// excess per plane instead of holding it in registers: 0.762 / 0.849 ms.
 #pragma once
 
 #include "blasm_cols.cuh"
 
 namespace cvqpg {
 
-constexpr int kC4G = 4;  // columns per CTA
+#ifndef CVQPG_COLS4_BPT
+#define CVQPG_COLS4_BPT 1
+#endif
+#ifndef CVQPG_COLS4_G
+#define CVQPG_COLS4_G 4
+#endif
+#ifdef CVQPG_COLS4_MAXNREG
+#define CVQPG_C4_BOUNDS(nt, mb) __maxnreg__(CVQPG_COLS4_MAXNREG)
+#else
+#define CVQPG_C4_BOUNDS(nt, mb) __launch_bounds__(nt, mb)
+#endif
+constexpr int kC4G = CVQPG_COLS4_G;      // adjacent columns per CTA
+constexpr int kC4Bpt = CVQPG_COLS4_BPT;  // radix-16 butterflies per thread
 
 template <int R2>
 struct Cols4Plan {
     static constexpr int N = 16 * R2 * 16;
     static constexpr int NB16 = N / 16;  // butterflies of a radix-16 pass per column
     static constexpr int NBR = N / R2;   // butterflies of the radix-R2 pass per column (256)
-    static constexpr int TPC = NB16 / 2;  // threads per column: two radix-16 butterflies each
+    static constexpr int BPT = kC4Bpt;
+    static constexpr int TPC = NB16 / BPT;  // threads per column
     static constexpr int NT = kC4G * TPC;
     static constexpr int RB = (NBR + TPC - 1) / TPC;  // radix-R2 butterflies per thread (rounds)
     static constexpr int LD = (N - 1 + ((N - 1) >> 4) + 1) * kC4G;  // float2 per shared buffer
     static constexpr int NTW = 256;  // twiddle prefix used (indices < 16 * 16 and < NB16)
     static constexpr size_t kSmem = (size_t)(2 * LD + NTW) * sizeof(float2);
+    static constexpr int kMinBlocks = kC4G == 2 ? 2 : 1;  // CTAs per SM the shared memory allows
 };
 
 __device__ __forceinline__ int c4_addr(int e, int g) { return (e + (e >> 4)) * kC4G + g; }
@@ -88,12 +107,14 @@ __device__ __forceinline__ void c4_last16(const float2* __restrict__ in, const f
     apply_twiddles<16>(v, w);
 }
 
-// Plane-independent transfer excess of the elements a thread holds (-1: no plane propagates it).
+// Plane-independent transfer excess of the elements a thread holds (-1: no plane
+// propagates it), kept in registers for all planes.
 template <int R2>
-__device__ __forceinline__ void c4_excess(const BlasmDev& d, int c, int ci, float bcol, int u, float (&E)[2][16]) {
+__device__ __forceinline__ void c4_excess(const BlasmDev& d, int c, int ci, float bcol, int u,
+                                          float (&E)[kC4Bpt][16]) {
     using PL = Cols4Plan<R2>;
 #pragma unroll
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < PL::BPT; b++) {
         const int j = u + b * PL::TPC;
 #pragma unroll
         for (int r = 0; r < 16; r++) {
@@ -122,7 +143,7 @@ __device__ __forceinline__ void c4_out16(const float2* __restrict__ in, const fl
                                          float2* __restrict__ dst, size_t ld, int row0, int nrows) {
     using PL = Cols4Plan<R2>;
 #pragma unroll
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < PL::BPT; b++) {
         const int j = u + b * PL::TPC;
         float2 v[16];
         c4_last16<R2, true>(in, tw, j, g, v);
@@ -143,9 +164,9 @@ template <int R2>
 __device__ __forceinline__ void c4_in16(const float2* __restrict__ src, size_t ld, int row0, int nrows,
                                         float2* __restrict__ out, int u, int g) {
     using PL = Cols4Plan<R2>;
-    float2 m[2][8];
+    float2 m[PL::BPT][8];
 #pragma unroll
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < PL::BPT; b++) {
         const int j = u + b * PL::TPC;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
@@ -154,7 +175,7 @@ __device__ __forceinline__ void c4_in16(const float2* __restrict__ src, size_t l
         }
     }
 #pragma unroll
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < PL::BPT; b++) {
         float2 v[16];
 #pragma unroll
         for (int i = 0; i < 8; i++) v[4 + i] = m[b][i];
@@ -166,7 +187,7 @@ __device__ __forceinline__ void c4_in16(const float2* __restrict__ src, size_t l
 // Forward: four columns of A [C][pH][NW] -> spectrum x transfer -> inverse per
 // plane -> the kept rows of B [P*C][out_h][NW].
 template <int R2>
-__global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_fwd_kernel(BlasmDev d,
+__global__ void CVQPG_C4_BOUNDS(Cols4Plan<R2>::NT, Cols4Plan<R2>::kMinBlocks) blasm_cols4_fwd_kernel(BlasmDev d,
                                                                               const float2* __restrict__ A,
                                                                               float2* __restrict__ B) {
     using PL = Cols4Plan<R2>;
@@ -174,7 +195,7 @@ __global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_fwd_kernel(B
     float2* b0 = sm;
     float2* b1 = sm + PL::LD;
     float2* tw = sm + 2 * PL::LD;
-    const int t = threadIdx.x, g = t & (kC4G - 1), u = t >> 2;
+    const int t = threadIdx.x, g = t & (kC4G - 1), u = t / kC4G;
     const int NW = d.NW, groups = NW / kC4G;
     const int c = blockIdx.x / groups, kx0 = (blockIdx.x - c * groups) * kC4G;
     for (int i = t; i < PL::NTW; i += PL::NT) tw[i] = __ldg(&d.col.tw[i]);
@@ -186,13 +207,13 @@ __global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_fwd_kernel(B
     int ci = kx0 + g + (NW >> 1);
     if (ci >= NW) ci -= NW;
     const float bcol = __ldg(&d.b_col[c * NW + ci]);
-    float2 spec[2][16];
-    float E[2][16];
+    float2 spec[PL::BPT][16];
 #pragma unroll
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < PL::BPT; b++) {
         c4_last16<R2, false>(b1, tw, u + b * PL::TPC, g, spec[b]);
         dft<16>(spec[b], false);
     }
+    float E[PL::BPT][16];
     c4_excess<R2>(d, c, ci, bcol, u, E);
     const int row0 = PL::N / 2 - d.out_h / 2, oh = d.out_h;
     for (int p = 0; p < d.P; p++) {
@@ -200,7 +221,7 @@ __global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_fwd_kernel(B
         const PCParam pp = d.pcp[pc];
         const bool col_ok = ci >= pp.i0 && ci < pp.i1;
 #pragma unroll
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < PL::BPT; b++) {
             const int j = u + b * PL::TPC;
             float2 v[16];
 #pragma unroll
@@ -219,7 +240,7 @@ __global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_fwd_kernel(B
 // Adjoint: per plane the forward transform of four columns of Bt [P*C][out_h][NW],
 // x conj(transfer) accumulated in registers; one inverse -> Ab [C][in_h][NW].
 template <int R2>
-__global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_adj_kernel(BlasmDev d,
+__global__ void CVQPG_C4_BOUNDS(Cols4Plan<R2>::NT, Cols4Plan<R2>::kMinBlocks) blasm_cols4_adj_kernel(BlasmDev d,
                                                                               const float2* __restrict__ Bt,
                                                                               float2* __restrict__ Ab) {
     using PL = Cols4Plan<R2>;
@@ -227,18 +248,18 @@ __global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_adj_kernel(B
     float2* b0 = sm;
     float2* b1 = sm + PL::LD;
     float2* tw = sm + 2 * PL::LD;
-    const int t = threadIdx.x, g = t & (kC4G - 1), u = t >> 2;
+    const int t = threadIdx.x, g = t & (kC4G - 1), u = t / kC4G;
     const int NW = d.NW, groups = NW / kC4G;
     const int c = blockIdx.x / groups, kx0 = (blockIdx.x - c * groups) * kC4G;
     for (int i = t; i < PL::NTW; i += PL::NT) tw[i] = __ldg(&d.col.tw[i]);
     int ci = kx0 + g + (NW >> 1);
     if (ci >= NW) ci -= NW;
     const float bcol = __ldg(&d.b_col[c * NW + ci]);
-    float E[2][16];
+    float E[PL::BPT][16];
     c4_excess<R2>(d, c, ci, bcol, u, E);
-    float2 acc[2][16];
+    float2 acc[PL::BPT][16];
 #pragma unroll
-    for (int b = 0; b < 2; b++)
+    for (int b = 0; b < PL::BPT; b++)
 #pragma unroll
         for (int r = 0; r < 16; r++) acc[b][r] = make_float2(0.f, 0.f);
     const int row0 = PL::N / 2 - d.out_h / 2, oh = d.out_h;
@@ -252,7 +273,7 @@ __global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_adj_kernel(B
         const PCParam pp = d.pcp[pc];
         const bool col_ok = ci >= pp.i0 && ci < pp.i1;
 #pragma unroll
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < PL::BPT; b++) {
             const int j = u + b * PL::TPC;
             float2 v[16];
             c4_last16<R2, false>(b1, tw, j, g, v);
@@ -264,7 +285,7 @@ __global__ void __launch_bounds__(Cols4Plan<R2>::NT, 1) blasm_cols4_adj_kernel(B
         }
     }
 #pragma unroll
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < PL::BPT; b++) {
         dft<16>(acc[b], true);
         c4_store16_stride1(b0, u + b * PL::TPC, g, acc[b]);
     }

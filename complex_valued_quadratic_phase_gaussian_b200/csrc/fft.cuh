@@ -169,16 +169,36 @@ __device__ __forceinline__ void dft(float2 (&v)[R], bool inv) {
     }
 }
 
-// v[r] *= w^r for r = 1..R-1, the powers formed by a running product: one
-// table load per butterfly instead of R-1 scattered ones, two live complex
-// values. The product chain adds at most R-2 roundings (~1e-6 relative at R=17).
-template <int R>
+// v[r] *= w^r for r = 1..R-1 from one table value w = w^1. The powers come
+// from a product tree, w^r = w^(2^k) * w^(r - 2^k) with 2^k the highest power
+// of two in r (and w^(2^k) = (w^(2^(k-1)))^2): R-2 products as in a running
+// product, but a dependency depth of about log2(R) instead of R-2, so the
+// butterfly does not wait on a serial chain, and at most ~2 log2(R) roundings.
+__device__ __forceinline__ float2 csqr(float2 a) {
+    return make_float2(fmaf(a.x, a.x, -a.y * a.y), 2.0f * a.x * a.y);
+}
+// TREE = false forms the powers by a running product instead (two live values
+// rather than R-1: for register-bound kernels).
+template <int R, bool TREE = true>
 __device__ __forceinline__ void apply_twiddles(float2 (&v)[R], float2 w1) {
-    float2 w = w1;
+    if constexpr (TREE) {
+        float2 pw[R];
+        pw[1] = w1;
 #pragma unroll
-    for (int r = 1; r < R; r++) {
-        v[r] = cmul(v[r], w);
-        if (r + 1 < R) w = cmul(w, w1);
+        for (int r = 2; r < R; r++) {
+            int hb = 1;
+            while (hb * 2 <= r) hb *= 2;
+            pw[r] = (r == hb) ? csqr(pw[r / 2]) : cmul(pw[hb], pw[r - hb]);
+        }
+#pragma unroll
+        for (int r = 1; r < R; r++) v[r] = cmul(v[r], pw[r]);
+    } else {
+        float2 w = w1;
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+            v[r] = cmul(v[r], w);
+            if (r + 1 < R) w = cmul(w, w1);
+        }
     }
 }
 
