@@ -78,6 +78,31 @@ __device__ __forceinline__ void sincos_reduced(float x, float* s, float* c) {
     __sincosf(r, s, c);
 }
 
+// The same SFU approximations through the PTX .ftz forms (ex2/sin/cos.approx.ftz.f32):
+// without .ftz the hardware approximations need fix-up instructions for denormal
+// arguments and results, which the splat paths never produce (|r| <= pi, and the
+// Gaussian factor is at least exp(-20) under the Mahalanobis cut).
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ void sincos_reduced_ftz(float x, float* s, float* c) {
+    const float kInv2Pi = 0.15915494309189535f;
+    const float k2PiHi = 6.28318548202514648f;
+    const float k2PiLo = -1.7484555314695172e-07f;
+    const float kRound = 12582912.0f;
+    const float n = __fsub_rn(__fmaf_rn(x, kInv2Pi, kRound), kRound);
+    float r = fmaf(-n, k2PiHi, x);
+    r = fmaf(-n, k2PiLo, r);
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(*s) : "f"(r));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(*c) : "f"(r));
+}
+
+// exp(-m / 2) = 2^(-m / (2 ln 2))
+constexpr float kNegHalfLog2e = -0.72134752044448170368f;
+
 // ---------------------------------------------------------------------------
 // Philox4x32-10 counter-based generator (J. K. Salmon, M. A. Moraes, R. O. Dror,
 // D. E. Shaw, "Parallel Random Numbers: As Easy as 1, 2, 3", SC 2011) and a

@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
             const float mahal = dx * (r0.z * dx + r0.w * dy) + dy * (r0.w * dx + r1.x * dy);
             if (!__any_sync(0xffffffffu, mahal < kMahalCut)) continue;
             const float power = fmaxf(-0.5f * mahal, -50.0f);
-            const float G = __expf(power);
+            const float G = ex2_ftz(power * 1.44269504088896341f);  // exp(power)
             // Mahalanobis QPF (c m area) or, with ISO, the isotropic form (c |r - mu|^2)
             const float base = ISO ? 0.5f * r1.z * (dx * dx + dy * dy) * dxy2 : 0.5f * r1.z * mahal * r1.w * dxy2;
             const float4 r2 = s_rec[j][2];
@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(kTilePixels) splat_forward_kernel(
 #pragma unroll
             for (int c = 0; c < C; c++) {
                 float s, co;
-                sincos_reduced(ph[c] + kc[c] * base, &s, &co);
+                sincos_reduced_ftz(ph[c] + kc[c] * base, &s, &co);
                 const float amp = col[c] * G;  // colour x opacity (folded at staging) x G
                 acc_r[c] = fmaf(amp, co, acc_r[c]);
                 acc_i[c] = fmaf(amp, s, acc_i[c]);
@@ -574,23 +574,6 @@ void launch_splat_forward(int channels, const BinRule& rule, const int32_t* rang
     }
 }
 
-// ---------------------------------------------------------------------------
-// splat adjoint: balanced over the active (Gaussian, pixel) pairs of a tile.
-// One CTA per tile. For a batch of list entries the CTA first computes, per
-// entry and tile row, the span of columns where the Mahalanobis distance is
-// under the cut (a quadratic in x, solved with a small outward margin; the
-// exact per-pixel test still applies), and a prefix over the entries' active
-// pixel counts. The flattened list of active pairs is then split into equal
-// contiguous ranges, one per thread, so every lane evaluates a live pixel on
-// every step instead of idling where its Gaussian does not reach. A thread's
-// per-Gaussian sums stay in registers until its range leaves that Gaussian,
-// then go to shared per-entry accumulators; one global atomic per parameter
-// per (Gaussian, tile) follows. Per-pixel terms are recomputed (same formulas
-// as cuda/backward.cu:101-147, including both paths of dL/dmahal).
-// ---------------------------------------------------------------------------
-constexpr int kBwdThreads = 128;
-constexpr int kBwdBatch = 256;  // list entries per batch
-
 // Columns [x0, x0 + n) of tile row `fy` (tile origin tx0, xmax columns) where
 // the Gaussian (mx, my, inverse covariance i00 i01 i11) may be under the cut.
 __device__ __forceinline__ void cut_row_span(float mx, float my, float i00, float i01, float i11, float fy, int tx0,
@@ -622,23 +605,60 @@ __device__ __forceinline__ void cut_row_span(float mx, float my, float i00, floa
     *n = (int)hi - (int)lo + 1;
 }
 
+// ---------------------------------------------------------------------------
+// splat adjoint over row segments ("items"): one CTA per tile. For a batch of
+// list entries the CTA cuts every entry's rows to the span under the
+// Mahalanobis cut (cut_row_span), and each non-empty (entry, row, span) is one
+// item. Items are counting-sorted by (span length descending, row), and thread
+// t takes items t, t + NT, ...: the 32 items of a warp step have (nearly) the
+// same length, and items of the same row read the same dL/dU pixels
+// (shared-memory broadcast).
+//
+// Along a row segment dy is fixed and dx steps by -1, so the Mahalanobis
+// distance is m = (i00 dx + 2 i01 dy) dx + i11 dy^2 and the per-pixel terms of
+// the reference adjoint (cuda/backward.cu:101-147) regroup into sums whose row
+// totals give every parameter. With (P_c + i Q_c) = conj(exp(i theta_c)) dL/dU_c:
+//   Acol_c = sum G P_c, Aph_c = sum G Q_c,
+//   M = G (-(1/2) sum_c col_c P_c + kq sum_c k_c col_c Q_c)   (= dL/dm / opacity,
+//       kq = c area dxy2 / 2),
+//   R0 = sum M, R1 = sum M dx, R2 = sum M dx^2, T = sum G (sum_c k_c col_c Q_c) m;
+// per row: d inv00 = o R2, d inv01 = 2 o dy R1, d inv11 = o dy^2 R0,
+// d mx = 2 o (i00 R1 + i01 dy R0), d my = 2 o (i11 dy R0 + i01 R1); per entry:
+// d opacity = sum_c col_c Acol_c, d colour_c = o Acol_c, d phase_c = o col_c Aph_c,
+// d curvature = o (area dxy2 / 2) T, d area = o (c dxy2 / 2) T (o = opacity).
+// The isotropic form (theta = phi + k (c dxy2 / 2)(dx^2 + dy^2)) has no phase
+// term in dL/dm and adds the phase's own dependence on the mean
+// (U0 = sum G K, U1 = sum G K dx, U2 = sum G K dx^2, K = sum_c k_c col_c Q_c).
+// The phase is evaluated per pixel (Cody-Waite reduction + SFU sin/cos), as in
+// the forward: a rotation recurrence along the row would save no issue slots
+// and its rounding drifts with the segment length.
+// ---------------------------------------------------------------------------
+constexpr int kRowThreads = 128;
+constexpr int kRowBatch = 96;                  // list entries per batch (one per thread in the cut pass)
+constexpr int kRowWarps = kRowThreads / 32;
+constexpr int kRowItems = kRowBatch * kTile;   // at most one item per entry and tile row
+constexpr int kRowKeys = kTile * kTile;        // sort keys: (16 - length) * 16 + row
+constexpr int kGRow = kTile + 1;               // padded row of the staged dL/dU tile
+
 template <int C, bool ISO>
-__global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
+__global__ void __launch_bounds__(kRowThreads) splat_backward_rows_kernel(
     BinRule rule, const int32_t* __restrict__ ranges, const int32_t* __restrict__ point_list,
     const float4* __restrict__ rec, const float* __restrict__ k, float dxy2, const float2* __restrict__ grad, int W,
     int H, int gx, SplatGrads out, const int32_t* __restrict__ order) {
-    constexpr int NA = 8 + 2 * C;  // dmx dmy d00 d01 d11 dop dcv dar dcol[C] dph[C]
-    constexpr int kWarps = kBwdThreads / 32;
-    constexpr int kPer = kBwdBatch / kBwdThreads;  // entries per thread in the span pass
-    __shared__ float2 s_g[C][kTilePixels];
-    // non-empty rows of each entry, in order: y | x0 << 4 | (n - 1) << 8
-    __shared__ uint16_t s_rows[kBwdBatch][kTile];
-    __shared__ uint8_t s_nr[kBwdBatch];
-    __shared__ int s_off[kBwdBatch + 1];
-    __shared__ int s_gid[kBwdBatch];  // Gaussian index of each entry of the batch
-    __shared__ float s_acc[NA][kBwdBatch];
-    __shared__ int s_wsum[kWarps];
-    static_assert(kBwdBatch % kBwdThreads == 0, "whole entries per thread");
+    constexpr int NV = (8 + 2 * C + 3) / 4;  // float4 words used per record
+    constexpr int NE = 6 + 2 * C;            // per-entry sums: mx my d00 d01 d11 T Acol[C] Aph[C]
+    __shared__ float2 s_g[C][kTile * kGRow];  // rows padded to 17: rows at one column hit distinct banks
+    __shared__ float4 s_rec[NV][kRowBatch];  // word-major: lanes of different entries hit distinct banks
+    __shared__ int s_gid[kRowBatch];
+    __shared__ uint32_t s_item[kRowItems];         // entry | row word << 8
+    // per-warp sums of each entry ([warp][NE][entry]); before the items are processed the same
+    // memory holds the entries' row spans and the sort-key counts
+    __shared__ float s_acc[kRowWarps * NE * kRowBatch];
+    // row word: 0 (empty) or 0x8000 | y | x0 << 4 | (n - 1) << 8
+    uint16_t(*s_rows)[kTile] = reinterpret_cast<uint16_t(*)[kTile]>(s_acc);
+    int* s_key = reinterpret_cast<int*>(s_acc) + kRowBatch * kTile / 2;
+    static_assert(kRowBatch * kTile / 2 + kRowKeys <= kRowWarps * NE * kRowBatch, "span and key scratch fit");
+    static_assert(kRowBatch <= kRowThreads, "one entry per thread in the cut pass");
 
     const int tile = order ? order[blockIdx.x] : blockIdx.x;
     const int2 range = reinterpret_cast<const int2*>(ranges)[list_of_tile(rule, tile % gx, tile / gx)];
@@ -646,11 +666,11 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     const int tx0 = (tile % gx) * kTile, ty0 = (tile / gx) * kTile;
     {  // the tile's dL/dU, all loads of a thread issued before its stores
-        constexpr int kIt = kTilePixels / kBwdThreads;
+        constexpr int kIt = kTilePixels / kRowThreads;
         float2 gv[kIt][C];
 #pragma unroll
         for (int u = 0; u < kIt; u++) {
-            const int p = t + u * kBwdThreads;
+            const int p = t + u * kRowThreads;
             const int px = tx0 + (p & 15), py = ty0 + (p >> 4);
             const bool inside = px < W && py < H;
             const size_t e = inside ? (size_t)py * W + px : 0;
@@ -660,243 +680,267 @@ __global__ void __launch_bounds__(kBwdThreads) splat_backward_kernel(
 #pragma unroll
         for (int u = 0; u < kIt; u++)
 #pragma unroll
-            for (int c = 0; c < C; c++) s_g[c][t + u * kBwdThreads] = gv[u][c];
+            for (int c = 0; c < C; c++) s_g[c][((t + u * kRowThreads) >> 4) * kGRow + ((t + u * kRowThreads) & 15)] = gv[u][c];
+        for (int i = t; i < C * kTile; i += kRowThreads) s_g[i / kTile][(i % kTile) * kGRow + kTile] = make_float2(0.f, 0.f);
     }
-    static_assert(kTilePixels % kBwdThreads == 0, "whole pixel rounds");
+    static_assert(kTilePixels % kRowThreads == 0, "whole pixel rounds");
     const int xmax = min(kTile, W - tx0), ymax = min(kTile, H - ty0);
 
     float kc[C];
 #pragma unroll
     for (int c = 0; c < C; c++) kc[c] = k[c];
 
-    for (int b0 = range.x; b0 < range.y; b0 += kBwdBatch) {
-        const int nb = min(kBwdBatch, range.y - b0);
-        // 1. spans and active counts; thread t owns entries kPer*t .. kPer*t + kPer-1
-        int cnt[kPer], gid[kPer];
-        float4 r0s[kPer];
-        float i11s[kPer];
-#pragma unroll
-        for (int u = 0; u < kPer; u++) gid[u] = kPer * t + u < nb ? point_list[b0 + kPer * t + u] : 0;
-#pragma unroll
-        for (int u = 0; u < kPer; u++) {
-            r0s[u] = __ldg(&rec[(size_t)gid[u] * 4 + 0]);
-            i11s[u] = __ldg(&rec[(size_t)gid[u] * 4 + 1]).x;
-        }
-#pragma unroll
-        for (int u = 0; u < kPer; u++) {
-            const int e = kPer * t + u;
-            cnt[u] = 0;
-            int nr = 0;
-            s_gid[e] = gid[u];
-            if (e < nb) {
-                const float4 r0 = r0s[u];
-                const float i11 = i11s[u];
-                for (int yy = 0; yy < ymax; yy++) {
-                    int x0, n;
-                    cut_row_span(r0.x, r0.y, r0.z, r0.w, i11, (float)(ty0 + yy), tx0, xmax, &x0, &n);
-                    if (n > 0) {
-                        s_rows[e][nr++] = (uint16_t)(yy | (x0 << 4) | ((n - 1) << 8));
-                        cnt[u] += n;
-                    }
-                }
-            }
-            s_nr[e] = (uint8_t)nr;
-#pragma unroll
-            for (int q = 0; q < NA; q++) s_acc[q][e] = 0.0f;
-        }
-        // 2. exclusive prefix of the counts in entry order
-        int local = 0;
-#pragma unroll
-        for (int u = 0; u < kPer; u++) local += cnt[u];
-        int incl = local;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) s_wsum[wid] = incl;
+    for (int b0 = range.x; b0 < range.y; b0 += kRowBatch) {
+        const int nb = min(kRowBatch, range.y - b0);
+        // 1. stage the entry's record and its row spans; count the sort keys
+        for (int i = t; i < kRowKeys; i += kRowThreads) s_key[i] = 0;
         __syncthreads();
-        int base = 0;
-        for (int w = 0; w < wid; w++) base += s_wsum[w];
-        int run = base + incl - local;
+        if (t < nb) {
+            const int g = point_list[b0 + t];
+            s_gid[t] = g;
 #pragma unroll
-        for (int u = 0; u < kPer; u++) {
-            s_off[kPer * t + u] = run;
-            run += cnt[u];
-        }
-        if (t == kBwdThreads - 1) s_off[kBwdBatch] = run;
-        __syncthreads();
-
-        // 3. this thread's contiguous share of the active pairs
-        const int total = s_off[kBwdBatch];
-        const int lo = (int)(((long long)total * t) / kBwdThreads);
-        const int hi = (int)(((long long)total * (t + 1)) / kBwdThreads);
-        if (lo < hi) {
-            int e = 0;  // last entry starting at or before lo
-            for (int step = kBwdBatch / 2; step > 0; step >>= 1)
-                if (e + step < nb && s_off[e + step] <= lo) e += step;
-            int k = 0, o = lo - s_off[e];
-            int w = s_rows[e][0];
-            while (o > (w >> 8)) {  // o >= row length
-                o -= (w >> 8) + 1;
-                w = s_rows[e][++k];
-            }
-            int nr = s_nr[e];
-            int r = w & 15, x = ((w >> 4) & 15) + o, rem = (w >> 8) + 1 - o;
-            float fx = (float)(tx0 + x), fy = (float)(ty0 + r);  // pixel coordinates, advanced in float
-
-            int g = s_gid[e];
-            float mx, my, i00, i01, i11, opac, curv, ar, kb, har, hcv, col[C], ph[C];
-            auto load = [&](int gg) {
-                const float4 r0 = __ldg(&rec[(size_t)gg * 4 + 0]);
-                const float4 r1 = __ldg(&rec[(size_t)gg * 4 + 1]);
-                const float4 r2 = __ldg(&rec[(size_t)gg * 4 + 2]);
-                mx = r0.x, my = r0.y, i00 = r0.z, i01 = r0.w, i11 = r1.x;
-                opac = r1.y, curv = r1.z, ar = r1.w;
-                kb = 0.5f * curv * ar * dxy2;  // dbase/dmahal
-                har = 0.5f * ar * dxy2;
-                hcv = 0.5f * curv * dxy2;
-                if (C == 1) {
-                    col[0] = r2.x;
-                    ph[0] = r2.y;
-                } else {
-                    const float4 r3 = __ldg(&rec[(size_t)gg * 4 + 3]);
-                    col[0] = r2.x;
-                    col[C > 1 ? 1 : 0] = r2.y;
-                    col[C > 2 ? 2 : 0] = r2.z;
-                    ph[0] = r2.w;
-                    ph[C > 1 ? 1 : 0] = r3.x;
-                    ph[C > 2 ? 2 : 0] = r3.y;
-                }
-            };
-            load(g);
-            float acc[NA];
-#pragma unroll
-            for (int q = 0; q < NA; q++) acc[q] = 0.0f;
-            auto flush = [&](int ee) {
-#pragma unroll
-                for (int q = 0; q < NA; q++) {
-                    if (acc[q] != 0.0f) atomicAdd(&s_acc[q][ee], acc[q]);
-                    acc[q] = 0.0f;
-                }
-            };
-
-            for (int it = lo; it < hi; it++) {
-                const float dx = mx - fx;
-                const float dy = my - fy;
-                const float mahal = dx * (i00 * dx + i01 * dy) + dy * (i01 * dx + i11 * dy);
-                if (mahal < kMahalCut) {
-                    // mahal < 40 here, so the forward's clamp of the exponent at -50 never applies
-                    // (and its derivative factor is -1/2)
-                    const float G = __expf(-0.5f * mahal);
-                    const float alpha = opac * G;
-                    const float d2 = dx * dx + dy * dy;
-                    const float base = ISO ? 0.5f * curv * d2 * dxy2 : 0.5f * curv * mahal * ar * dxy2;
-                    const int p = r * kTile + x;
-                    float S_alpha = 0.f, S_base = 0.f;
-#pragma unroll
-                    for (int c = 0; c < C; c++) {
-                        float s, co;
-                        sincos_reduced(ph[c] + kc[c] * base, &s, &co);
-                        const float2 gp = s_g[c][p];
-                        const float proj_c = gp.x * co + gp.y * s;
-                        const float proj_s = -gp.x * s + gp.y * co;
-                        const float aph = col[c] * alpha * proj_s;
-                        acc[8 + c] = fmaf(alpha, proj_c, acc[8 + c]);
-                        acc[8 + C + c] += aph;
-                        S_alpha = fmaf(col[c], proj_c, S_alpha);
-                        S_base = fmaf(kc[c], aph, S_base);
-                    }
-                    const float dpow = -0.5f;
-                    float dmahal;
-                    if (ISO) {
-                        // the phase reaches the means directly: dbase/dmu = c dxy2 (mu - r)
-                        dmahal = S_alpha * opac * G * dpow;
-                        acc[6] = fmaf(S_base, 0.5f * d2 * dxy2, acc[6]);
-                        acc[0] = fmaf(S_base * curv * dxy2, dx, acc[0]);
-                        acc[1] = fmaf(S_base * curv * dxy2, dy, acc[1]);
-                    } else {
-                        dmahal = S_alpha * opac * G * dpow + S_base * kb;
-                        acc[6] = fmaf(S_base * mahal, har, acc[6]);
-                        acc[7] = fmaf(S_base * mahal, hcv, acc[7]);
-                    }
-                    acc[2] = fmaf(dmahal, dx * dx, acc[2]);
-                    acc[3] = fmaf(dmahal, 2.0f * dx * dy, acc[3]);
-                    acc[4] = fmaf(dmahal, dy * dy, acc[4]);
-                    acc[0] = fmaf(dmahal, 2.0f * (i00 * dx + i01 * dy), acc[0]);
-                    acc[1] = fmaf(dmahal, 2.0f * (i11 * dy + i01 * dx), acc[1]);
-                    acc[5] = fmaf(S_alpha, G, acc[5]);
-                }
-                // advance to the next active pixel of this entry, or to the next entry
-                x++;
-                fx += 1.0f;
-                if (--rem == 0) {
-                    if (++k == nr) {
-                        flush(e);
-                        if (it + 1 >= hi) break;
-                        e++;
-                        while (e + 1 < nb && s_off[e + 1] == s_off[e]) e++;  // skip entries with no active pixel
-                        g = s_gid[e];
-                        load(g);
-                        nr = s_nr[e];
-                        k = 0;
-                    }
-                    w = s_rows[e][k];
-                    r = w & 15;
-                    x = (w >> 4) & 15;
-                    rem = (w >> 8) + 1;
-                    fx = (float)(tx0 + x);
-                    fy = (float)(ty0 + r);
-                }
-            }
-            flush(e);  // no-op when the range ended on an entry boundary (sums already cleared)
+            for (int q = 0; q < NV; q++) s_rec[q][t] = __ldg(&rec[(size_t)g * 4 + q]);
         }
         __syncthreads();
-        // 4. one global atomic per parameter per (Gaussian, tile)
-        for (int e = t; e < nb; e += kBwdThreads) {
-            const int g = s_gid[e];
-            float v[NA];
+        // spans, one (entry, row) per thread step (16 lanes share an entry: broadcast reads)
+        for (int idx = t; idx < nb * kTile; idx += kRowThreads) {
+            const int e = idx >> 4, yy = idx & 15;
+            const float4 r0 = s_rec[0][e];
+            const float i11 = s_rec[1][e].x;
+            int x0 = 0, n = 0;
+            // a Gaussian whose mean or inverse covariance is not finite reaches no pixel under the cut
+            const bool finite = fabsf(r0.x) + fabsf(r0.y) + fabsf(r0.z) + fabsf(r0.w) + fabsf(i11) < INFINITY;
+            if (finite && yy < ymax) cut_row_span(r0.x, r0.y, r0.z, r0.w, i11, (float)(ty0 + yy), tx0, xmax, &x0, &n);
+            s_rows[e][yy] = n > 0 ? (uint16_t)(0x8000 | yy | (x0 << 4) | ((n - 1) << 8)) : (uint16_t)0;
+            if (n > 0) atomicAdd(&s_key[(kTile - n) * kTile + yy], 1);
+        }
+        __syncthreads();
+        // 2. exclusive scan of the key counts (warp 0; 8 keys per lane)
+        if (wid == 0) {
+            constexpr int kPerLane = kRowKeys / 32;
+            int cnt[kPerLane], sum = 0;
 #pragma unroll
-            for (int q = 0; q < NA; q++) v[q] = s_acc[q][e];
-            if (v[0] != 0.f) atomicAdd(&out.d_means[2 * g], v[0]);
-            if (v[1] != 0.f) atomicAdd(&out.d_means[2 * g + 1], v[1]);
-            if (v[2] != 0.f) atomicAdd(&out.d_inv[3 * g], v[2]);
-            if (v[3] != 0.f) atomicAdd(&out.d_inv[3 * g + 1], v[3]);
-            if (v[4] != 0.f) atomicAdd(&out.d_inv[3 * g + 2], v[4]);
-            if (v[5] != 0.f) atomicAdd(&out.d_op[g], v[5]);
-            if (v[6] != 0.f) atomicAdd(&out.d_cv[g], v[6]);
-            if (v[7] != 0.f) atomicAdd(&out.d_ar[g], v[7]);
+            for (int u = 0; u < kPerLane; u++) {
+                cnt[u] = s_key[lane * kPerLane + u];
+                sum += cnt[u];
+            }
+            int incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            int run = incl - sum;
+#pragma unroll
+            for (int u = 0; u < kPerLane; u++) {
+                s_key[lane * kPerLane + u] = run;
+                run += cnt[u];
+            }
+        }
+        __syncthreads();
+        // 3. scatter the items into key order
+        for (int idx = t; idx < nb * kTile; idx += kRowThreads) {
+            const int w = s_rows[idx >> 4][idx & 15];
+            if (w & 0x8000) {
+                const int n = ((w >> 8) & 15) + 1, yy = w & 15;
+                const int pos = atomicAdd(&s_key[(kTile - n) * kTile + yy], 1);
+                s_item[pos] = (uint32_t)(idx >> 4) | ((uint32_t)(w & 0xfff) << 8);
+            }
+        }
+        __syncthreads();
+        const int nitems = s_key[kRowKeys - 1];  // the last key's cursor ends at the item total
+        __syncthreads();  // every thread holds the total before the scratch becomes the sums
+        for (int i = t; i < kRowWarps * NE * kRowBatch; i += kRowThreads) s_acc[i] = 0.0f;
+        __syncthreads();
+
+        // 4. the items, 32 per warp step (warp-uniform loop: the flush below needs the whole warp)
+        float* acc = s_acc + wid * (NE * kRowBatch);
+        for (int base = wid * 32; base < nitems; base += kRowThreads) {
+            const int i = base + lane;
+            const bool valid = i < nitems;
+            const uint32_t word = s_item[valid ? i : 0];
+            const int e = word & 0xff;
+            const int yy = (word >> 8) & 15, x0 = (word >> 12) & 15;
+            const int n = valid ? ((word >> 16) & 15) + 1 : 0;
+            const float4 r0 = s_rec[0][e], r1 = s_rec[1][e], r2 = s_rec[2][e];
+            const float mx = r0.x, my = r0.y, i00 = r0.z, i01 = r0.w, i11 = r1.x;
+            const float curv = r1.z, ar = r1.w;
+            float col[C], ph[C];
+            if (C == 1) {
+                col[0] = r2.x;
+                ph[0] = r2.y;
+            } else {
+                const float4 r3 = s_rec[NV - 1][e];
+                col[0] = r2.x;
+                col[C > 1 ? 1 : 0] = r2.y;
+                col[C > 2 ? 2 : 0] = r2.z;
+                ph[0] = r2.w;
+                ph[C > 1 ? 1 : 0] = r3.x;
+                ph[C > 2 ? 2 : 0] = r3.y;
+            }
+            const float fy = (float)(ty0 + yy);
+            const float dy = my - fy;
+            float dx = mx - (float)(tx0 + x0);
+            const float lin = 2.0f * i01 * dy, cst = i11 * dy * dy;  // m = (i00 dx + lin) dx + cst
+            // phase = phi_c + k_c base, base = kq m (isotropic form: kq (dx^2 + dy^2))
+            const float kq = ISO ? 0.5f * curv * dxy2 : 0.5f * curv * ar * dxy2;
+            const float dy2 = dy * dy;
+            float kcol[C], colh[C];
 #pragma unroll
             for (int c = 0; c < C; c++) {
-                if (v[8 + c] != 0.f) atomicAdd(&out.d_col[g * C + c], v[8 + c]);
-                if (v[8 + C + c] != 0.f) atomicAdd(&out.d_ph[g * C + c], v[8 + C + c]);
+                kcol[c] = kc[c] * col[c];
+                colh[c] = -0.5f * col[c];
+            }
+            float acol[C], aph[C];
+#pragma unroll
+            for (int c = 0; c < C; c++) acol[c] = aph[c] = 0.0f;
+            float R0 = 0.f, R1 = 0.f, R2 = 0.f, T = 0.f, U0 = 0.f, U1 = 0.f, U2 = 0.f;
+            int p = yy * kGRow + x0;
+#pragma unroll 2
+            for (int j = 0; j < n; j++, p++) {
+                const float mahal = fmaf(fmaf(i00, dx, lin), dx, cst);
+                {
+                    // a pixel beyond the cut adds nothing (G = 0; its terms are finite). Under the cut
+                    // mahal < 40, so the forward's clamp of the exponent at -50 never applies.
+                    const float G = mahal < kMahalCut ? ex2_ftz(mahal * kNegHalfLog2e) : 0.0f;
+                    const float base = kq * (ISO ? fmaf(dx, dx, dy2) : mahal);
+                    float sp = 0.f, kqs = 0.f;
+#pragma unroll
+                    for (int c = 0; c < C; c++) {
+                        float zs, zc;
+                        sincos_reduced_ftz(fmaf(kc[c], base, ph[c]), &zs, &zc);
+                        const float2 gp = s_g[c][p];
+                        const float P = fmaf(gp.x, zc, gp.y * zs);
+                        const float Q = fmaf(gp.y, zc, -gp.x * zs);
+                        acol[c] = fmaf(G, P, acol[c]);
+                        aph[c] = fmaf(G, Q, aph[c]);
+                        sp = fmaf(colh[c], P, sp);
+                        kqs = fmaf(kcol[c], Q, kqs);
+                    }
+                    const float gk = G * kqs;
+                    if (ISO) {
+                        const float M = G * sp;
+                        const float tm = M * dx;
+                        R0 += M;
+                        R1 += tm;
+                        R2 = fmaf(tm, dx, R2);
+                        const float tu = gk * dx;
+                        U0 += gk;
+                        U1 += tu;
+                        U2 = fmaf(tu, dx, U2);
+                    } else {
+                        const float M = fmaf(kq, gk, G * sp);
+                        const float tm = M * dx;
+                        R0 += M;
+                        R1 += tm;
+                        R2 = fmaf(tm, dx, R2);
+                        T = fmaf(gk, mahal, T);
+                    }
+                }
+                dx -= 1.0f;
+            }
+            // the row's totals into the entry's sums (opacity factors applied per entry)
+            float v[NE];
+            v[0] = 2.0f * fmaf(i00, R1, i01 * dy * R0);
+            v[1] = 2.0f * fmaf(i11 * dy, R0, i01 * R1);
+            v[2] = R2;
+            v[3] = 2.0f * dy * R1;
+            v[4] = dy2 * R0;
+            if (ISO) {
+                const float hc = curv * dxy2;
+                v[0] = fmaf(hc, U1, v[0]);
+                v[1] = fmaf(hc * dy, U0, v[1]);
+                v[5] = 0.5f * dxy2 * fmaf(dy2, U0, U2);
+            } else {
+                v[5] = T;
+            }
+#pragma unroll
+            for (int c = 0; c < C; c++) {
+                v[6 + c] = acol[c];
+                v[6 + C + c] = aph[c];
+            }
+            // Into this warp's sums: a float atomicAdd on shared memory is a compare-and-swap loop,
+            // so lanes that share an entry add in turn instead (rank among the lanes with that entry).
+            __syncwarp();
+            const unsigned peers = __match_any_sync(0xffffffffu, valid ? (unsigned)e : 0x100u + (unsigned)lane);
+            const int rank = __popc(peers & ((1u << lane) - 1u));
+            const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
+            for (int r = 0; r < rounds; r++) {
+                if (valid && rank == r) {
+#pragma unroll
+                    for (int q = 0; q < NE; q++) acc[q * kRowBatch + e] += v[q];
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // 5. one global atomic per parameter per (Gaussian, tile)
+        if (t < nb) {
+            const int g = s_gid[t];
+            const float4 r1 = s_rec[1][t], r2 = s_rec[2][t];
+            const float opac = r1.y, curv = r1.z, ar = r1.w;
+            float col[C];
+            col[0] = r2.x;
+            if (C > 1) {
+                col[C > 1 ? 1 : 0] = r2.y;
+                col[C > 2 ? 2 : 0] = r2.z;
+            }
+            float a[NE];
+#pragma unroll
+            for (int q = 0; q < NE; q++) {
+                a[q] = 0.0f;
+#pragma unroll
+                for (int w = 0; w < kRowWarps; w++) a[q] += s_acc[(w * NE + q) * kRowBatch + t];
+            }
+            float dop = 0.0f;
+#pragma unroll
+            for (int c = 0; c < C; c++) dop = fmaf(col[c], a[6 + c], dop);
+            const float vm0 = opac * a[0], vm1 = opac * a[1];
+            const float v00 = opac * a[2], v01 = opac * a[3], v11 = opac * a[4];
+            const float vcv = ISO ? opac * a[5] : opac * (0.5f * ar * dxy2) * a[5];
+            const float var = ISO ? 0.0f : opac * (0.5f * curv * dxy2) * a[5];
+            if (vm0 != 0.f) atomicAdd(&out.d_means[2 * g], vm0);
+            if (vm1 != 0.f) atomicAdd(&out.d_means[2 * g + 1], vm1);
+            if (v00 != 0.f) atomicAdd(&out.d_inv[3 * g], v00);
+            if (v01 != 0.f) atomicAdd(&out.d_inv[3 * g + 1], v01);
+            if (v11 != 0.f) atomicAdd(&out.d_inv[3 * g + 2], v11);
+            if (dop != 0.f) atomicAdd(&out.d_op[g], dop);
+            if (vcv != 0.f) atomicAdd(&out.d_cv[g], vcv);
+            if (var != 0.f) atomicAdd(&out.d_ar[g], var);
+#pragma unroll
+            for (int c = 0; c < C; c++) {
+                const float vc = opac * a[6 + c], vp = opac * col[c] * a[6 + C + c];
+                if (vc != 0.f) atomicAdd(&out.d_col[g * C + c], vc);
+                if (vp != 0.f) atomicAdd(&out.d_ph[g * C + c], vp);
             }
         }
         __syncthreads();
     }
 }
 
+template <int C, bool ISO>
+static void launch_splat_backward_t(const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
+                                    const float4* rec, const float* k, float dxy2, const float2* grad,
+                                    const SplatGrads& out, cudaStream_t stream, const int32_t* tile_order) {
+    const int gx = (rule.width + kTile - 1) / kTile, gy = (rule.height + kTile - 1) / kTile;
+    splat_backward_rows_kernel<C, ISO><<<gx * gy, kRowThreads, 0, stream>>>(
+        rule, ranges, point_list, rec, k, dxy2, grad, rule.width, rule.height, gx, out, tile_order);
+}
+
 void launch_splat_backward(int channels, const BinRule& rule, const int32_t* ranges, const int32_t* point_list,
                            const float* records, const float* k, float dxy2, const float2* grad,
                            const SplatGrads& out, cudaStream_t stream, bool iso, const int32_t* tile_order) {
-    const int width = rule.width, height = rule.height;
-    const int gx = (width + kTile - 1) / kTile, gy = (height + kTile - 1) / kTile;
     const float4* rec = reinterpret_cast<const float4*>(records);
-    const dim3 grid(gx * gy);
     if (channels == 1) {
         if (iso)
-            splat_backward_kernel<1, true><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                             grad, width, height, gx, out, tile_order);
+            launch_splat_backward_t<1, true>(rule, ranges, point_list, rec, k, dxy2, grad, out, stream, tile_order);
         else
-            splat_backward_kernel<1, false><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                              grad, width, height, gx, out, tile_order);
+            launch_splat_backward_t<1, false>(rule, ranges, point_list, rec, k, dxy2, grad, out, stream, tile_order);
     } else {
         if (iso)
-            splat_backward_kernel<3, true><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                             grad, width, height, gx, out, tile_order);
+            launch_splat_backward_t<3, true>(rule, ranges, point_list, rec, k, dxy2, grad, out, stream, tile_order);
         else
-            splat_backward_kernel<3, false><<<grid, kBwdThreads, 0, stream>>>(rule, ranges, point_list, rec, k, dxy2,
-                                                                              grad, width, height, gx, out, tile_order);
+            launch_splat_backward_t<3, false>(rule, ranges, point_list, rec, k, dxy2, grad, out, stream, tile_order);
     }
 }
 
