@@ -100,6 +100,12 @@ __device__ __forceinline__ void sincos_reduced_ftz(float x, float* s, float* c) 
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(*c) : "f"(r));
 }
 
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // exp(-m / 2) = 2^(-m / (2 ln 2))
 constexpr float kNegHalfLog2e = -0.72134752044448170368f;
 

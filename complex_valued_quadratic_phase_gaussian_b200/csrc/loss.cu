@@ -202,7 +202,9 @@ __global__ void __launch_bounds__(kLossThreads, NM == 3 ? 4 : 3) loss_kernel(Los
                 const float s11 = exx - mu1 * mu1, s22 = eyy - mu2 * mu2, s12 = exy - mu1 * mu2;
                 const float A1 = 2.f * mu1 * mu2 + C1, A2 = 2.f * s12 + C2;
                 const float B1 = mu1 * mu1 + mu2 * mu2 + C1, B2 = s11 + s22 + C2;
-                const float iB1 = 1.f / B1, iB2 = 1.f / B2;
+                // B1 >= C1 and B2 >= C2 (positive constants): the SFU reciprocal (within 1 ulp) needs no
+                // IEEE special cases
+                const float iB1 = rcp_ftz(B1), iB2 = rcp_ftz(B2);
                 const float smap = A1 * A2 * iB1 * iB2;
                 if (ii >= 10 && jj >= 10) ssim_sum += smap;  // owned map position
                 dm = 2.f * mu2 * A2 * iB1 * iB2 - 2.f * mu1 * smap * iB1 +

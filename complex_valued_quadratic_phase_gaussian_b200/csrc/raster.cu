@@ -651,9 +651,11 @@ __global__ void __launch_bounds__(kRowThreads) splat_backward_rows_kernel(
     __shared__ float4 s_rec[NV][kRowBatch];  // word-major: lanes of different entries hit distinct banks
     __shared__ int s_gid[kRowBatch];
     __shared__ uint32_t s_item[kRowItems];         // entry | row word << 8
-    // per-warp sums of each entry ([warp][NE][entry]); before the items are processed the same
+    // per-warp sums of each entry ([warp][entry][NE], NE a multiple of 4: one lane's sums are three
+    // float4 words at a 48-byte stride, eight bank groups); before the items are processed the same
     // memory holds the entries' row spans and the sort-key counts
-    __shared__ float s_acc[kRowWarps * NE * kRowBatch];
+    __shared__ __align__(16) float s_acc[kRowWarps * NE * kRowBatch];
+    static_assert(NE % 4 == 0, "per-entry sums in float4 words");
     // row word: 0 (empty) or 0x8000 | y | x0 << 4 | (n - 1) << 8
     uint16_t(*s_rows)[kTile] = reinterpret_cast<uint16_t(*)[kTile]>(s_acc);
     int* s_key = reinterpret_cast<int*>(s_acc) + kRowBatch * kTile / 2;
@@ -868,7 +870,15 @@ __global__ void __launch_bounds__(kRowThreads) splat_backward_rows_kernel(
             for (int r = 0; r < rounds; r++) {
                 if (valid && rank == r) {
 #pragma unroll
-                    for (int q = 0; q < NE; q++) acc[q * kRowBatch + e] += v[q];
+                    for (int q = 0; q < NE / 4; q++) {
+                        float4* a4 = reinterpret_cast<float4*>(acc + e * NE) + q;
+                        float4 x = *a4;
+                        x.x += v[4 * q];
+                        x.y += v[4 * q + 1];
+                        x.z += v[4 * q + 2];
+                        x.w += v[4 * q + 3];
+                        *a4 = x;
+                    }
                 }
                 __syncwarp();
             }
@@ -887,11 +897,17 @@ __global__ void __launch_bounds__(kRowThreads) splat_backward_rows_kernel(
             }
             float a[NE];
 #pragma unroll
-            for (int q = 0; q < NE; q++) {
-                a[q] = 0.0f;
+            for (int q = 0; q < NE; q++) a[q] = 0.0f;
 #pragma unroll
-                for (int w = 0; w < kRowWarps; w++) a[q] += s_acc[(w * NE + q) * kRowBatch + t];
-            }
+            for (int w = 0; w < kRowWarps; w++)
+#pragma unroll
+                for (int q = 0; q < NE / 4; q++) {
+                    const float4 x = reinterpret_cast<const float4*>(s_acc + (w * kRowBatch + t) * NE)[q];
+                    a[4 * q] += x.x;
+                    a[4 * q + 1] += x.y;
+                    a[4 * q + 2] += x.z;
+                    a[4 * q + 3] += x.w;
+                }
             float dop = 0.0f;
 #pragma unroll
             for (int c = 0; c < C; c++) dop = fmaf(col[c], a[6 + c], dop);
