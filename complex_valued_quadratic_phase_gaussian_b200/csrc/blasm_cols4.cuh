@@ -184,6 +184,43 @@ __device__ __forceinline__ void c4_in16(const float2* __restrict__ src, size_t l
     }
 }
 
+// The adjoint's per-plane input block (the out_h kept rows x four columns, row-major, 32 B per
+// row) is copied into a shared staging buffer with cp.async while the previous plane computes.
+constexpr int kC4StageRows = 1216;  // staging capacity in rows (the shared memory left by the two buffers)
+
+__device__ __forceinline__ void c4_stage_async(float2* __restrict__ stage, const float2* __restrict__ src, size_t ld,
+                                               int nrows, int t, int nt) {
+    // 16-byte chunks: two per row (columns g = 0,1 and 2,3)
+    for (int i = t; i < 2 * nrows; i += nt) {
+        const int y = i >> 1, h = i & 1;
+        const float2* s = src + (size_t)y * ld + 2 * h;
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(stage + 4 * y + 2 * h);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(s) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void c4_stage_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// c4_in16 reading the staged block (rows y = e - row0 in [0, nrows) at stage[4 y + g]).
+template <int R2>
+__device__ __forceinline__ void c4_in16_staged(const float2* __restrict__ stage, int row0, int nrows,
+                                               float2* __restrict__ out, int u, int g) {
+    using PL = Cols4Plan<R2>;
+#pragma unroll
+    for (int b = 0; b < PL::BPT; b++) {
+        const int j = u + b * PL::TPC;
+        float2 v[16];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int y = j + (4 + i) * PL::NB16 - row0;
+            v[4 + i] = (unsigned)y < (unsigned)nrows ? stage[4 * y + g] : make_float2(0.f, 0.f);
+        }
+        dft16_mid_in(v, false);
+        c4_store16_stride1(out, j, g, v);
+    }
+}
+
 // Forward: four columns of A [C][pH][NW] -> spectrum x transfer -> inverse per
 // plane -> the kept rows of B [P*C][out_h][NW].
 template <int R2>
@@ -263,11 +300,23 @@ __global__ void CVQPG_C4_BOUNDS(Cols4Plan<R2>::NT, Cols4Plan<R2>::kMinBlocks) bl
 #pragma unroll
         for (int r = 0; r < 16; r++) acc[b][r] = make_float2(0.f, 0.f);
     const int row0 = PL::N / 2 - d.out_h / 2, oh = d.out_h;
+    // the next plane's input is staged while this plane computes (when its rows fit)
+    float2* stage = sm + 2 * PL::LD + PL::NTW;
+    const bool staged = oh <= kC4StageRows;
+    if (staged) c4_stage_async(stage, Bt + (size_t)c * oh * NW + kx0, NW, oh, t, PL::NT);
     for (int p = 0; p < d.P; p++) {
         const int pc = p * d.C + c;
         // b0 was last read by the previous plane's radix-R2 pass, before its closing barrier
-        c4_in16<R2>(Bt + (size_t)pc * oh * NW + kx0, NW, row0, oh, b0, u, g);
+        if (staged) {
+            c4_stage_wait();
+            __syncthreads();
+            c4_in16_staged<R2>(stage, row0, oh, b0, u, g);
+        } else {
+            c4_in16<R2>(Bt + (size_t)pc * oh * NW + kx0, NW, row0, oh, b0, u, g);
+        }
         __syncthreads();
+        if (staged && p + 1 < d.P)  // every thread has read the stage (barrier above)
+            c4_stage_async(stage, Bt + (size_t)(pc + d.C) * oh * NW + kx0, NW, oh, t, PL::NT);
         c4_pass_mid<R2, false>(b0, b1, tw, u, g);
         __syncthreads();
         const PCParam pp = d.pcp[pc];
@@ -305,8 +354,9 @@ void launch_cols4_t(bool adjoint, const BlasmDev& d, const float2* in, float2* o
         cudaFuncSetAttribute(blasm_cols4_fwd_kernel<R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::kSmem);
         blasm_cols4_fwd_kernel<R2><<<grid, PL::NT, PL::kSmem, s>>>(d, in, out);
     } else {
-        cudaFuncSetAttribute(blasm_cols4_adj_kernel<R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::kSmem);
-        blasm_cols4_adj_kernel<R2><<<grid, PL::NT, PL::kSmem, s>>>(d, in, out);
+        const size_t smem = PL::kSmem + (size_t)kC4StageRows * kC4G * sizeof(float2);
+        cudaFuncSetAttribute(blasm_cols4_adj_kernel<R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        blasm_cols4_adj_kernel<R2><<<grid, PL::NT, smem, s>>>(d, in, out);
     }
 }
 
