@@ -546,8 +546,10 @@ def run_time_to_psnr():
     res["training"] = {"wall_seconds": round(train_s, 2), "pairs": info["pairs"],
                        "fits": "2 rounds x 64 fits of 256x256 crops with 1080p statistics, 400 iterations, "
                                "batched fitter; round 2 starts from round 1's network",
-                       "mlp": "1024-512-512-156 GELU, BF16 tcgen05 GEMMs, FP32 Adam, 3000 steps x 8192 tiles",
-                       "final_loss": info["loss_round2"][-1][1]}
+                       "mlp": "1024-512-512-156 GELU, BF16 tcgen05 GEMMs, FP32 Adam, 3000 steps x 8192 tiles; 10 % "
+                              "of the fits held out, the weights of the best validation loss kept",
+                       "final_loss": info["loss_round2"]["train"][-1][1],
+                       "best_validation_loss": info["loss_round2"]["best_val"]}
     res["note"] = ("times are fit-iteration device time (CUDA events, every iteration), evaluation excluded; "
                    "the learned and constant fits are checked against the goal after every iteration; 'learned' "
                    "includes the network's prediction; 'constant' is the ablation without the network (every slot "

@@ -180,17 +180,39 @@ def output_weights(T):
     return (1.0 / var).repeat(SLOTS).float().contiguous()
 
 
-def train(X, T, steps=2000, batch=8192, lr=3e-4, seed=0, log_every=0):
-    """Fit a TileMLP to (X, T) with Adam on minibatches; returns (net, output weights, loss curve)."""
+def train(X, T, steps=2000, batch=8192, lr=3e-4, seed=0, log_every=0, val_fraction=0.1, val_every=0):
+    """Fit a TileMLP to (X, T) with Adam on minibatches; returns (net, output weights, loss curve).
+
+    The last `val_fraction` of the rows (whole scenes: make_pairs stacks them scene by scene) are held
+    out. Every `val_every` steps (default steps / 20) the weighted validation loss is measured and the
+    net keeps the weights of the best one (early stopping: longer training overfits the training
+    scenes). The curve holds (step, train loss) pairs and, under "val", (step, validation loss)."""
     dev = X.device
-    n = X.shape[0]
+    n_all = X.shape[0]
+    n_val = int(n_all * val_fraction) if val_fraction > 0 else 0
+    n = n_all - n_val
     batch = min(batch, n)
     net = TileMLP(batch, IN_DIM, 512, OUT_DIM, lr=lr, device=dev)
-    wout = output_weights(T)
+    wout = output_weights(T[:n])
     g = torch.Generator(device=dev).manual_seed(seed)
     xb = torch.empty((batch, IN_DIM), dtype=torch.float32, device=dev)
     tb = torch.empty((batch, OUT_DIM), dtype=torch.float32, device=dev)
-    curve = []
+    curve, val_curve = [], []
+    if n_val > 0:
+        val_every = val_every or max(1, steps // 20)
+        chunk = min(batch, n_val)
+        n_val -= n_val % chunk
+        val_net = TileMLP(chunk, IN_DIM, 512, OUT_DIM, weights=net.weights, device=dev)  # shares net.weights
+        best, best_loss = net.weights.clone(), float("inf")
+
+    def validate():
+        val_net.sync()
+        tot = torch.zeros((), dtype=torch.float64, device=dev)
+        for a in range(n, n + n_val, chunk):
+            y = val_net.forward(X[a:a + chunk])
+            tot += (((y - T[a:a + chunk]) ** 2) * wout).sum(dtype=torch.float64)
+        return float(tot) / max(n_val, 1)
+
     for it in range(steps):
         idx = torch.randint(0, n, (batch,), generator=g, device=dev)
         torch.index_select(X, 0, idx, out=xb)
@@ -198,6 +220,16 @@ def train(X, T, steps=2000, batch=8192, lr=3e-4, seed=0, log_every=0):
         loss = net.train_step(xb, tb, wout)
         if log_every and (it % log_every == 0 or it == steps - 1):
             curve.append((it, float(loss.item())))
+        if n_val > 0 and ((it + 1) % val_every == 0 or it == steps - 1):
+            v = validate()
+            val_curve.append((it, v))
+            if v < best_loss:
+                best_loss = v
+                best.copy_(net.weights)
+    if n_val > 0:
+        net.weights.copy_(best)
+        net.sync()
+        curve = dict(train=curve, val=val_curve, best_val=best_loss)
     return net, wout, curve
 
 
