@@ -193,14 +193,12 @@ __device__ __forceinline__ void c4_stage_async(float2* __restrict__ stage, const
     // 16-byte chunks: two per row (columns g = 0,1 and 2,3)
     for (int i = t; i < 2 * nrows; i += nt) {
         const int y = i >> 1, h = i & 1;
-        const float2* s = src + (size_t)y * ld + 2 * h;
-        const uint32_t d = (uint32_t)__cvta_generic_to_shared(stage + 4 * y + 2 * h);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(s) : "memory");
+        cp_async16(stage + 4 * y + 2 * h, src + (size_t)y * ld + 2 * h);
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+    cp_async_commit();
 }
 
-__device__ __forceinline__ void c4_stage_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void c4_stage_wait() { cp_async_wait_all(); }
 
 // c4_in16 reading the staged block (rows y = e - row0 in [0, nrows) at stage[4 y + g]).
 template <int R2>

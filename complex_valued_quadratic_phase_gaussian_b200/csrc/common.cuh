@@ -106,6 +106,14 @@ __device__ __forceinline__ float rcp_ftz(float x) {
     return y;
 }
 
+// Asynchronous 16-byte global -> shared copies (cp.async, completion by wait_group).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // exp(-m / 2) = 2^(-m / (2 ln 2))
 constexpr float kNegHalfLog2e = -0.72134752044448170368f;
 
