@@ -188,10 +188,10 @@ def test_isotropic_phase_vs_reference_torch_renderer(golden):
 
 @pytest.mark.parametrize("iso", [False, True])
 def test_adjoint_thin_gaussians_ragged_tiles_vs_float64_oracle(iso):
-    """The splat adjoint balances each tile's pairs over its threads through per-row spans of the
-    Mahalanobis cut. Thin, rotated Gaussians (spans of a pixel or two, rows with none), Gaussians
-    past the image border and a 70 x 45 image (ragged edge tiles) against the float64 oracle on
-    the same lists: every gradient within 1e-4 relative L2."""
+    """The splat adjoint works on per-row spans of the Mahalanobis cut (length-sorted segments).
+    Thin, rotated Gaussians (spans of a pixel or two, rows with none), Gaussians past the image
+    border and a 70 x 45 image (ragged edge tiles) against the float64 oracle on the same lists:
+    every gradient within 1e-4 relative L2."""
     from complex_valued_quadratic_phase_gaussian_b200.rasterizer import render_backward, render_forward
     rng = np.random.default_rng(21 + iso)
     n, W, H, C = 300, 70, 45, 3
@@ -227,3 +227,54 @@ def test_adjoint_thin_gaussians_ragged_tiles_vs_float64_oracle(iso):
         if iso and name == "d_ar":
             continue  # the isotropic phase does not use the area
         assert rel_l2(a, b) < 1e-4, (name, rel_l2(a, b))
+
+
+@pytest.mark.parametrize("C,iso", [(3, False), (1, False), (3, True)])
+def test_adjoint_long_lists_over_many_batches_vs_float64_oracle(C, iso):
+    """Tiles whose lists hold several batches of entries (the adjoint stages 96 per batch): 700
+    Gaussians of 0.6-5 px, 500 of them within 10 px of one point, so the tiles around it list
+    hundreds of entries, the same Gaussian often several times per batch in one warp's segments.
+    Large curvatures (the phase turns quickly along a row). Every gradient within 1e-4 relative L2
+    of the float64 oracle on the same lists, and the lists are those of the oracle's binning."""
+    from complex_valued_quadratic_phase_gaussian_b200.rasterizer import render_backward, render_forward
+    rng = np.random.default_rng(7 + C + 10 * iso)
+    n, W, H = 700, 80, 56
+    centre = np.array([37.0, 29.0])
+    means = np.concatenate([centre + rng.normal(0, 5.0, (500, 2)),
+                            np.stack([rng.uniform(0, W, 200), rng.uniform(0, H, 200)], 1)]).astype(np.float32)
+    s = rng.uniform(0.6, 5.0, (n, 2))
+    th = rng.uniform(0, np.pi, n)
+    c, si = np.cos(th), np.sin(th)
+    c00 = s[:, 0] ** 2 * c * c + s[:, 1] ** 2 * si * si + 0.05
+    c01 = (s[:, 0] ** 2 - s[:, 1] ** 2) * c * si
+    c11 = s[:, 0] ** 2 * si * si + s[:, 1] ** 2 * c * c + 0.05
+    det = c00 * c11 - c01 ** 2
+    inv = np.stack([c11 / det, -c01 / det, c00 / det], 1).astype(np.float32)
+    radii = osp.radius5_int(c00, c01, c11)
+    col = rng.uniform(0, 1, (n, C)).astype(np.float32)
+    ph = rng.uniform(0, 2 * np.pi, (n, C)).astype(np.float32)
+    op = rng.uniform(0.2, 0.9, n).astype(np.float32)
+    cv = rng.normal(0, 1500, n).astype(np.float32)
+    ar = (s[:, 0] * s[:, 1]).astype(np.float32)
+    wl = [639e-9, 515e-9, 473e-9][:C] if C == 3 else [515e-9]
+    k = (2 * np.pi / np.array(wl)).astype(np.float32)
+    dxy2 = 3.74e-6 ** 2
+    T = [torch.from_numpy(a).cuda() for a in (means, inv, col, ph, op, cv, ar)]
+    K = torch.from_numpy(k).cuda()
+    _, pl, ranges = render_forward(*T, K, dxy2, W, H, radii=torch.from_numpy(radii).cuda(), phase_iso=iso)
+    pl_ref, ranges_ref = osp.bin_lists(means, W, H, osp.CULL_CUDA16_5SIGMA, radii=radii)
+    assert np.array_equal(pl.cpu().numpy()[:len(pl_ref)], pl_ref)
+    lens = ranges_ref[:, 1] - ranges_ref[:, 0]
+    assert lens.max() > 3 * 96, lens.max()
+    g = (rng.normal(size=(C, H, W)) + 1j * rng.normal(size=(C, H, W))).astype(np.complex64)
+    got = render_backward(torch.from_numpy(g).cuda(), *T, K, pl, ranges, dxy2, W, H, phase_iso=iso)
+    ref = osp.splat_backward(g, means, inv, col, ph, op, cv, ar, k, dxy2, W, H, cull=osp.CULL_CUDA16_5SIGMA,
+                             point_list=pl_ref, ranges=ranges_ref, phase_iso=iso)
+    names = ("d_means", "d_inv", "d_col", "d_ph", "d_op", "d_cv", "d_ar")
+    for name, a, b in zip(names, got, ref):
+        if iso and name == "d_ar":
+            continue
+        a = a.cpu().numpy().astype(np.float64).reshape(b.shape)
+        e = rel_l2(a, b)
+        print(f"long lists C={C} iso={iso} {name}: rel-L2 {e:.2e}")
+        assert e < 1e-4, (name, e)
