@@ -1,16 +1,17 @@
-// BF16 GEMM on the sm_100a tensor cores: TMA -> shared memory (4-stage ring,
+// BF16 GEMM on the sm_100a tensor cores: TMA -> shared memory (3-stage ring,
 // 128-byte swizzle) -> tcgen05.mma into a TMEM accumulator -> tcgen05.ld ->
 // fused epilogue (bias, GELU, GELU derivative, BF16 row-major and transposed
 // copies, split-K slabs).
 //
-// One CTA computes one 128 x 128 tile of C with 4 warps:
+// One CTA computes one 128 x 128 tile of C with 8 warps, two CTAs per SM:
 //   warp 0, lane 0: TMA producer (waits for a free stage, arms its mbarrier with
 //                   the byte count, issues the A and B tile loads);
 //   warp 1, lane 0: MMA issuer (waits for a full stage, issues 4 MMAs of K = 16,
 //                   commits to the stage's "empty" barrier; after the last stage
 //                   commits to the "done" barrier); warp 1 also owns the TMEM
 //                   allocation (128 columns);
-//   all 4 warps:    epilogue; warp w reads TMEM lanes 32w..32w+31 (= rows of C).
+//   all 8 warps:    epilogue; warp w reads TMEM lanes 32 (w % 4) .. +31 (= rows of C),
+//                   warps w and w + 4 take the two halves of the columns.
 // Each thread of the epilogue owns one row of C, so stores of the transposed
 // copy (column-major) are coalesced across the warp.
 //
@@ -24,8 +25,22 @@
 
 namespace cvqpg {
 
-constexpr int kGemmStages = 4;
-constexpr int kGemmThreads = 128;
+// 3 stages of 32 KB let two CTAs share an SM, so one CTA's epilogue overlaps the other's main
+// loop (measured on the MLP's 8192-row GEMMs: 4 stages at one CTA per SM took 44 / 38 us for the
+// 1024- / 512-deep forward layers, 3 stages at two CTAs 32 / 28 us, with 8 warps 29 / 25 us)
+#ifndef CVQPG_GEMM_STAGES
+#define CVQPG_GEMM_STAGES 3
+#endif
+#ifndef CVQPG_GEMM_CTAS_PER_SM
+#define CVQPG_GEMM_CTAS_PER_SM 2
+#endif
+#ifndef CVQPG_GEMM_THREADS
+#define CVQPG_GEMM_THREADS 256
+#endif
+constexpr int kGemmStages = CVQPG_GEMM_STAGES;
+constexpr int kGemmThreads = CVQPG_GEMM_THREADS;  // 128 or 256: warps w and w + 4 share TMEM lane quadrant w
+constexpr int kEpiGroups = kGemmThreads / 128;     // column groups of the epilogue
+static_assert(kGemmThreads == 128 || kGemmThreads == 256, "one or two warps per TMEM lane quadrant");
 constexpr uint32_t kStageBytesA = kGemmBM * kGemmBK * 2;  // 16 KB
 constexpr uint32_t kStageBytesB = kGemmBN * kGemmBK * 2;  // 16 KB
 constexpr size_t kGemmSmem = 1024 /* alignment slack */ + kGemmStages * (kStageBytesA + kStageBytesB) + 256;
@@ -62,8 +77,22 @@ __device__ __forceinline__ void gemm_epilogue16(const GemmEpi& e, int m, int n0,
         }
     } else {  // CVQPG_GEMM_EPI_DGELU: dZ = acc * gelu'(Z)
         const float* z = e.zin + (size_t)m * e.ld_z + n0;
+        float zz[16];
+        if (((e.ld_z & 3) | (int)((uintptr_t)e.zin & 15)) == 0) {  // the lane's 16 values as four float4 loads
 #pragma unroll
-        for (int j = 0; j < 16; j++) h[j] = (n0 + j < e.valid_n) ? v[j] * gelu_grad(__ldg(&z[j])) : 0.0f;
+            for (int j = 0; j < 16; j += 4) {
+                const float4 q = __ldg(reinterpret_cast<const float4*>(z + j));
+                zz[j] = q.x;
+                zz[j + 1] = q.y;
+                zz[j + 2] = q.z;
+                zz[j + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) zz[j] = __ldg(&z[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 16; j++) h[j] = (n0 + j < e.valid_n) ? v[j] * gelu_grad(zz[j]) : 0.0f;
     }
     if (e.out_bf16) {
         __align__(16) __nv_bfloat16 b[16];
@@ -79,7 +108,7 @@ __device__ __forceinline__ void gemm_epilogue16(const GemmEpi& e, int m, int n0,
     }
 }
 
-__global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
+__global__ void __launch_bounds__(kGemmThreads, CVQPG_GEMM_CTAS_PER_SM) tc_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
                                                                   const __grid_constant__ CUtensorMap map_b,
                                                                   int kblocks, GemmEpi epi, int* status) {
     extern __shared__ uint8_t gsm_raw[];
@@ -157,11 +186,14 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
 
     if (!mbar_wait(done, 0)) atomicExch(status, 3);
     tc_fence_after();
-    const int m = m0 + warp * 32 + lane;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    // warp w reads TMEM lanes 32 (w % 4) .. +31 (its quadrant); with 8 warps the two warps of a
+    // quadrant take alternate halves of the columns
+    const int quad = warp & 3, cg = warp >> 2;
+    const int m = m0 + quad * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16);
     if (complete) {
 #pragma unroll 1
-        for (int c0 = 0; c0 < kGemmBN; c0 += 16) {
+        for (int c0 = cg * (kGemmBN / kEpiGroups); c0 < (cg + 1) * (kGemmBN / kEpiGroups); c0 += 16) {
             float v[16];
             tmem_ld16(trow + (uint32_t)c0, v);
             gemm_epilogue16(epi, m, n0 + c0, blockIdx.z, v);
