@@ -140,7 +140,9 @@ def test_rgb_1080p_compile_time_plans_match_run_time_plans():
 def test_rgb_1080p_padded_input_four_and_one_column_kernels_agree():
     """input_mode 1 (an already padded field, as the POH reconstruction uses) with the full padded
     output at the 1080p grid: the four-column kernels keep every row of the middle half; forward and
-    adjoint agree with the one-column kernels (CVQPG_PLAN_COLS1) within 1e-5 relative L2."""
+    adjoint agree with the one-column kernels (CVQPG_PLAN_COLS1) within 1e-5 relative L2. With 1408
+    kept rows the four-column adjoint reads each plane's input straight from global memory (the
+    fit's 1080-row crops are staged in shared memory instead, covered by the fit and BLASM tests)."""
     from complex_valued_quadratic_phase_gaussian_b200.propagator import (BlasmPlan, reference_distances,
                                                                          reference_pad_size)
     rng = np.random.default_rng(8)
