@@ -156,13 +156,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(stage):
-    """DRAM bytes per launch of a stage from a committed ncu summary (profiles/*.md), or None."""
+def profiled_traffic(stage, workload="rgb1080"):
+    """DRAM bytes per launch of a stage from a committed ncu summary (profiles/*_<workload>.md), or
+    None: the summaries hold captures of one workload, and another workload's launch moves other bytes."""
     pdir = os.path.join(REPO, "profiles")
     if not os.path.isdir(pdir):
         return None
     for name in sorted(os.listdir(pdir)):
-        if not name.endswith(".md"):
+        if not name.endswith(f"_{workload}.md"):
             continue
         with open(os.path.join(pdir, name)) as f:
             for line in f:
@@ -389,7 +390,7 @@ def run_ours(args, wl, dist, world, rank, local):
     dom = max(hbm_stages, key=hbm_stages.get)
     peak, peak_kind = measured_peaks()
     achieved = nbytes[dom] / (stage_ms[dom] / 1e3) / 1e9
-    traffic = profiled_traffic(dom)
+    traffic = profiled_traffic(dom, args.workload)
 
     # end to end through the public API with pinned host buffers
     pinned_t = targets.cpu().pin_memory()
