@@ -612,7 +612,9 @@ __device__ __forceinline__ void cut_row_span(float mx, float my, float i00, floa
 // item. Items are counting-sorted by (span length descending, row), and thread
 // t takes items t, t + NT, ...: the 32 items of a warp step have (nearly) the
 // same length, and items of the same row read the same dL/dU pixels
-// (shared-memory broadcast).
+// (shared-memory broadcast). Each warp adds its items' sums into its own
+// per-entry sums in shared memory; one global atomic per parameter per
+// (Gaussian, tile) follows at the end of the batch.
 //
 // Along a row segment dy is fixed and dx steps by -1, so the Mahalanobis
 // distance is m = (i00 dx + 2 i01 dy) dx + i11 dy^2 and the per-pixel terms of
@@ -634,7 +636,7 @@ __device__ __forceinline__ void cut_row_span(float mx, float my, float i00, floa
 // and its rounding drifts with the segment length.
 // ---------------------------------------------------------------------------
 constexpr int kRowThreads = 128;
-constexpr int kRowBatch = 96;                  // list entries per batch (one per thread in the cut pass)
+constexpr int kRowBatch = 96;                  // list entries per batch (one per thread when staging)
 constexpr int kRowWarps = kRowThreads / 32;
 constexpr int kRowItems = kRowBatch * kTile;   // at most one item per entry and tile row
 constexpr int kRowKeys = kTile * kTile;        // sort keys: (16 - length) * 16 + row
@@ -660,7 +662,7 @@ __global__ void __launch_bounds__(kRowThreads) splat_backward_rows_kernel(
     uint16_t(*s_rows)[kTile] = reinterpret_cast<uint16_t(*)[kTile]>(s_acc);
     int* s_key = reinterpret_cast<int*>(s_acc) + kRowBatch * kTile / 2;
     static_assert(kRowBatch * kTile / 2 + kRowKeys <= kRowWarps * NE * kRowBatch, "span and key scratch fit");
-    static_assert(kRowBatch <= kRowThreads, "one entry per thread in the cut pass");
+    static_assert(kRowBatch <= kRowThreads, "one entry per thread when staging the records");
 
     const int tile = order ? order[blockIdx.x] : blockIdx.x;
     const int2 range = reinterpret_cast<const int2*>(ranges)[list_of_tile(rule, tile % gx, tile / gx)];
