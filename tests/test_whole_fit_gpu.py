@@ -1,13 +1,14 @@
-"""GPU: a whole fit, not single iterations. From the bench's 1920x1080 RGB start (96,000
-random-init Gaussians, 3 planes, seed 0), 2000 iterations of the fused fit (graph replays) and
-2000 iterations of the reference loop on the same GPU: its own CUDA rasterizer (compiled from its
-sources, oracle/_ref) under the torch propagator, loss + SSIM and Adan of
-train_2d_gaussian_rgb.py:147-262 (oracle/torch_port.py, pinned to the loop goldens), with the
-loop's own target noise (torch.randn_like, utils/propagator.py:432) where the fused fit draws its
-counter-based noise. The trajectories are never re-synchronised, so the gates are on outcomes:
-the noise-free per-plane PSNR of both final parameter sets, evaluated by the same kernel, within
-GATE_DB, and the two loss curves within LOSS_GATE (relative) at iterations 250, 1000 and 2000.
-The reference loop takes about two minutes here.
+"""GPU: a whole fit, not single iterations. From the bench's start (1920x1080 RGB, 96,000
+random-init Gaussians, 3 planes; and the 256x256 gray c0 case, 4096 Gaussians, 3 planes; seed 0),
+2000 iterations of the fused fit (graph replays) and 2000 iterations of the reference loop on the
+same GPU: its own CUDA rasterizer (compiled from its sources, oracle/_ref) under the torch
+propagator, loss + SSIM and Adan of train_2d_gaussian_rgb.py:147-262 (oracle/torch_port.py,
+pinned to the loop goldens), with the loop's own target noise (torch.randn_like,
+utils/propagator.py:432) where the fused fit draws its counter-based noise. The trajectories are
+never re-synchronised, so the gates are on outcomes: the noise-free per-plane PSNR of both final
+parameter sets, evaluated by the same kernel, within GATE_DB, and the two loss curves within
+LOSS_GATE (relative) at iterations 250, 1000 and 2000. The 1080p reference loop takes about two
+minutes here.
 """
 import numpy as np
 import pytest
@@ -16,25 +17,30 @@ import torch
 pytestmark = pytest.mark.gpu
 RAW = ("means_2d", "pre_act_scales", "pre_act_rotation", "colours", "pre_act_phase", "pre_act_opacities",
        "curvature")
-W, H, N, P = 1920, 1080, 96000, 3
-WAVELENGTHS = [639e-9, 515e-9, 473e-9]
+CASES = {
+    "rgb1080": dict(W=1920, H=1080, N=96000, P=3, wl=[639e-9, 515e-9, 473e-9], pitch=3.74e-6, d_val=1e-3),
+    "gray256": dict(W=256, H=256, N=4096, P=3, wl=[515e-9], pitch=8e-6, d_val=1.5e-3),
+}
 ITERS = 2000
 CHECK = (250, 1000, 2000)
 GATE_DB = 0.2
 LOSS_GATE = 0.03
 
 
-def test_whole_fit_reaches_the_reference_loops_psnr():
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_whole_fit_reaches_the_reference_loops_psnr(case):
     from complex_valued_quadratic_phase_gaussian_b200 import scenes
     from complex_valued_quadratic_phase_gaussian_b200.fit import FitConfig, Fitter, synthetic_init
     from oracle.torch_port import ReferencePipeline, load_reference_extension
     ext = load_reference_extension()
     if ext is None:
         pytest.skip("reference extension not built (oracle/build_ref.py needs the reference sources)")
-    img, depth = scenes.rgb_blobs(H, W, seed=0)
+    c = CASES[case]
+    W, H, P = c["W"], c["H"], c["P"]
+    img, depth = (scenes.rgb_blobs(H, W, seed=0) if len(c["wl"]) == 3 else scenes.grayscale_blobs(H, W, seed=0))
     targets, q = scenes.multiplane_targets_device(img, depth, P, device="cuda")
-    cfg = FitConfig(img_size=(W, H), num_gaussians=N, wavelengths=list(WAVELENGTHS), pixel_pitch=3.74e-6,
-                    num_planes=P, d_val=1e-3, volume_depth=1e-3, warmup_iters=400, num_itrs=ITERS, seed=0)
+    cfg = FitConfig(img_size=(W, H), num_gaussians=c["N"], wavelengths=list(c["wl"]), pixel_pitch=c["pitch"],
+                    num_planes=P, d_val=c["d_val"], volume_depth=1e-3, warmup_iters=400, num_itrs=ITERS, seed=0)
     init = synthetic_init(cfg, 0)
 
     f = Fitter(cfg, targets, q, init=init)
@@ -58,8 +64,8 @@ def test_whole_fit_reaches_the_reference_loops_psnr():
     f.load_raw({k: pipe.params[k].detach() for k in RAW})
     ref_eval = f.evaluate()
 
-    print("whole fit, loss (ours / reference):", {it: (round(ours[it], 6), round(ref[it], 6)) for it in CHECK})
-    print("whole fit, final PSNR per plane: ours", np.round(ours_eval["psnr"], 3), "reference",
+    print(f"whole fit {case}, loss (ours / reference):", {it: (round(ours[it], 6), round(ref[it], 6)) for it in CHECK})
+    print(f"whole fit {case}, final PSNR per plane: ours", np.round(ours_eval["psnr"], 3), "reference",
           np.round(ref_eval["psnr"], 3))
     assert np.all(np.isfinite(ours_eval["psnr"])) and np.all(np.isfinite(ref_eval["psnr"]))
     for it in CHECK:
