@@ -106,12 +106,111 @@ __global__ void __launch_bounds__(256) adan_kernel(AdanDev A) {
     }
 }
 
+// The same update in one pass over all tensors, four elements per thread with float4 accesses,
+// for the fit's layout: every array (parameters, gradients, each state vector) holds the tensors
+// back to back at the same offsets. end[t] = the flat index one past tensor t. Elements of a
+// tensor that does not step this iteration are written back unchanged; the per-element arithmetic
+// and its order are those of adan_kernel.
+struct AdanFlat {
+    int end[kParamTensors];
+    int total;
+};
+__global__ void __launch_bounds__(256) adan_flat4_kernel(AdanDev A, AdanFlat F) {
+    const int i0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (i0 >= F.total) return;
+    const float clip = A.scalars[0];
+    const float b1 = (float)A.beta1, b2 = (float)A.beta2, b3 = (float)A.beta3;
+    const float ob1 = (float)(1.0 - A.beta1), ob2 = (float)(1.0 - A.beta2), ob3 = (float)(1.0 - A.beta3);
+    const float eps = (float)A.eps;
+    float4 G4 = *reinterpret_cast<const float4*>(A.grad[0] + i0);
+    float4 M4 = *reinterpret_cast<const float4*>(A.exp_avg[0] + i0);
+    float4 V4 = *reinterpret_cast<const float4*>(A.exp_avg_sq[0] + i0);
+    float4 D4 = *reinterpret_cast<const float4*>(A.exp_avg_diff[0] + i0);
+    float4 N4 = *reinterpret_cast<const float4*>(A.neg_pre_grad[0] + i0);
+    float4 P4 = *reinterpret_cast<const float4*>(A.param[0] + i0);
+    float* Gv = &G4.x;
+    float* Mv = &M4.x;
+    float* Vv = &V4.x;
+    float* Dv = &D4.x;
+    float* Nv = &N4.x;
+    float* Pv = &P4.x;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int i = i0 + e;
+        int t = 0;
+#pragma unroll
+        for (int k = 0; k < kParamTensors - 1; k++) t += i >= F.end[k] ? 1 : 0;
+        const float* sc = A.scalars + 8 + 8 * t;
+        if (sc[0] == 0.0f) continue;
+        const bool fresh = sc[1] != 0.0f;
+        const float step_size = sc[2], step_size_diff = sc[3], bc3f = sc[4], wd = sc[5];
+        float g = Gv[e] * clip;
+        float m = fresh ? 0.f : Mv[e], v = fresh ? 0.f : Vv[e], d = fresh ? 0.f : Dv[e];
+        float ng = fresh ? -g : Nv[e];
+        ng = ng + g;
+        m = m * b1 + ob1 * g;
+        d = d * b2 + ob2 * ng;
+        ng = ng * b2 + g;
+        v = v * b3 + ob3 * ng * ng;
+        const float denom = sqrtf(v) / bc3f + eps;
+        float p = Pv[e];
+        if (A.no_prox) {
+            p = p * (1.0f - wd);
+            p = p + (-step_size) * (m / denom);
+            p = p + (-step_size_diff) * (d / denom);
+        } else {
+            p = p + (-step_size) * (m / denom);
+            p = p + (-step_size_diff) * (d / denom);
+            p = p / (1.0f + wd);
+        }
+        Pv[e] = p;
+        Mv[e] = m;
+        Vv[e] = v;
+        Dv[e] = d;
+        Nv[e] = -g;
+        Gv[e] = g;
+    }
+    *reinterpret_cast<float4*>(A.grad[0] + i0) = G4;
+    *reinterpret_cast<float4*>(A.exp_avg[0] + i0) = M4;
+    *reinterpret_cast<float4*>(A.exp_avg_sq[0] + i0) = V4;
+    *reinterpret_cast<float4*>(A.exp_avg_diff[0] + i0) = D4;
+    *reinterpret_cast<float4*>(A.neg_pre_grad[0] + i0) = N4;
+    *reinterpret_cast<float4*>(A.param[0] + i0) = P4;
+}
+
+// True when the tensors are back to back in every array and the flat arrays allow float4 access.
+static bool adan_flat_layout(const AdanDev& A, AdanFlat* F) {
+    long long off = 0;
+    for (int t = 0; t < kParamTensors; t++) {
+        float* const arrs[6] = {A.param[t], A.grad[t], A.exp_avg[t], A.exp_avg_sq[t], A.exp_avg_diff[t],
+                                A.neg_pre_grad[t]};
+        float* const bases[6] = {A.param[0], A.grad[0], A.exp_avg[0], A.exp_avg_sq[0], A.exp_avg_diff[0],
+                                 A.neg_pre_grad[0]};
+        for (int k = 0; k < 6; k++)
+            if (arrs[k] != bases[k] + off) return false;
+        off += A.numel[t];
+        F->end[t] = (int)off;
+    }
+    if (off % 4 != 0 || off > 0x7fffffffLL) return false;
+    F->total = (int)off;
+    float* const bases[6] = {A.param[0], A.grad[0], A.exp_avg[0], A.exp_avg_sq[0], A.exp_avg_diff[0],
+                             A.neg_pre_grad[0]};
+    for (int k = 0; k < 6; k++)
+        if ((uintptr_t)bases[k] & 15) return false;
+    return true;
+}
+
 void launch_adan(const AdanDev& A, const int32_t* iteration, cudaStream_t s) {
     int maxn = 1;
     for (int t = 0; t < kParamTensors; t++) maxn = max(maxn, A.numel[t]);
     const unsigned bx = min(ceil_div(maxn, 256), 4096u);
     dim3 grid(bx, kParamTensors);
     adan_scalars_kernel<<<1, 32, 0, s>>>(A, iteration);
+    AdanFlat F;
+    if (adan_flat_layout(A, &F)) {
+        adan_flat4_kernel<<<ceil_div((size_t)F.total / 4, 256), 256, 0, s>>>(A, F);
+        return;
+    }
     adan_kernel<<<grid, 256, 0, s>>>(A);
 }
 
