@@ -8,9 +8,13 @@ counter-based target noise (the oracle's restatement of the generator); at 1080p
 restatement is too slow on the host, it draws its own noise (torch.randn_like,
 utils/propagator.py:432) from a seeded generator. The trajectories are never re-synchronised, so
 the gates are on outcomes: the noise-free per-plane PSNR of both final
-parameter sets, evaluated by the same kernel, within GATE_DB, and the two loss curves within
-LOSS_GATE (relative) at iterations 250, 1000 and 2000. The 1080p reference loop takes about two
-minutes here.
+parameter sets, evaluated by the same kernel, within `db`, and the two loss curves within `loss`
+(relative) at iterations 250, 1000 and 2000. Both loops sum gradients with float atomics, so
+neither run repeats bit for bit, and the gates sit at about twice the reference loop's own
+spread across repeated runs, measured on this B200: at 1080p its final PSNR moved by 0.03 dB; at
+256x256 with 4096 Gaussians its final plane-3 PSNR ranged 32.58-32.81 dB over four runs (two of
+them on identical noise) and its loss at iteration 2000 0.00267-0.00280. The 1080p reference loop
+takes about two minutes here.
 """
 import numpy as np
 import pytest
@@ -21,13 +25,12 @@ RAW = ("means_2d", "pre_act_scales", "pre_act_rotation", "colours", "pre_act_pha
        "curvature")
 CASES = {
     "rgb1080": dict(W=1920, H=1080, N=96000, P=3, wl=[639e-9, 515e-9, 473e-9], pitch=3.74e-6, d_val=1e-3,
-                    same_noise=False),
-    "gray256": dict(W=256, H=256, N=4096, P=3, wl=[515e-9], pitch=8e-6, d_val=1.5e-3, same_noise=True),
+                    same_noise=False, db=0.2, loss=0.03),
+    "gray256": dict(W=256, H=256, N=4096, P=3, wl=[515e-9], pitch=8e-6, d_val=1.5e-3, same_noise=True, db=0.5,
+                    loss=0.08),
 }
 ITERS = 2000
 CHECK = (250, 1000, 2000)
-GATE_DB = 0.2
-LOSS_GATE = 0.03
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
@@ -76,5 +79,5 @@ def test_whole_fit_reaches_the_reference_loops_psnr(case):
           np.round(ref_eval["psnr"], 3))
     assert np.all(np.isfinite(ours_eval["psnr"])) and np.all(np.isfinite(ref_eval["psnr"]))
     for it in CHECK:
-        assert abs(ours[it] - ref[it]) <= LOSS_GATE * ref[it], (it, ours[it], ref[it])
-    assert np.max(np.abs(ours_eval["psnr"] - ref_eval["psnr"])) <= GATE_DB, (ours_eval["psnr"], ref_eval["psnr"])
+        assert abs(ours[it] - ref[it]) <= c["loss"] * ref[it], (it, ours[it], ref[it])
+    assert np.max(np.abs(ours_eval["psnr"] - ref_eval["psnr"])) <= c["db"], (ours_eval["psnr"], ref_eval["psnr"])
